@@ -1,0 +1,484 @@
+#!/usr/bin/env python
+"""Cone-beam forward + backprojection throughput (GUPS) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload cone512|cone256] [--storage bf16|fp16|fp32]
+
+One step = ConeProjection3D of a 512^3 (or 256^3) volume followed by
+ConeBackprojection3D of the resulting sinogram (360 views), the north-star
+workload.  GUPS = 2 U / t with U = voxels x views (the update count of one
+backprojection, used for both directions as the metric defines it).
+
+* ``value``: device-resident inputs, CUDA events around exactly K steps,
+  max over ranks; N ranks each run their own volume (weak scaling, no
+  data-path collective).
+* ``e2e``: the same step through the public API (pyronn_layers ops) with the
+  volume copied from pinned host memory and the result copied back inside the
+  timed region.
+* ``roofline``: the dominant kernel's algorithmic gather bytes (8 taps per
+  forward ray sample, 4 taps per backprojection update, times the storage
+  element size, plus its output bytes) over its live CUDA-event time, against
+  the measured HBM copy bandwidth.  Values above 1 mean the gathers are served
+  on chip (L1 / texture / L2) rather than from HBM.
+* ``cpu_baseline``: the FP64 CPU oracle (C, all host threads) on a bounded
+  sample (some views, some z-slices), scaled to the full step.
+* ``--impl reference``: the CPU oracle as the reference arm (the reference
+  has no CPU implementation of these ops; its CUDA kernels are the oracle's
+  parity target), same metric and config.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import datetime
+import io
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "pyro-nn-layers_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "cone-beam fwd+back GUPS, BF16 vs plain FP32 at ≤1e-3 rel err; serving p50/p99"
+
+WORKLOADS = {
+    "cone512": dict(volume=(512, 512, 512), voxel_mm=0.5, detector=(768, 1024), pixel_mm=1.0, views=360,
+                    sid_mm=750.0, sdd_mm=1200.0, step_voxels=0.5),
+    "cone256": dict(volume=(256, 256, 256), voxel_mm=0.5, detector=(512, 512), pixel_mm=1.0, views=360,
+                    sid_mm=750.0, sdd_mm=1200.0, step_voxels=0.5),
+}
+PHANTOM_ELLIPSOIDS = 32
+L2_BYTES = 126 * 1024 * 1024
+
+
+# ------------------------------------------------------------ helpers (CPU-testable)
+
+
+def shard_seed(base_seed: int, rank: int) -> int:
+    """Each rank backprojects its own volume: the phantom seed of rank r."""
+    return base_seed + 1000 * rank
+
+
+def aggregate(per_rank_ms, units_per_rank, steps):
+    """Whole-job throughput: all ranks' units over the slowest rank's time."""
+    t = max(per_rank_ms) / 1e3
+    return units_per_rank * len(per_rank_ms) * steps / t
+
+
+def updates(cfg) -> int:
+    z, y, x = cfg["volume"]
+    return z * y * x * cfg["views"]
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def decompose_np(P, spacing_zyx, origin_zyx):
+    """FP64 camera centre / inverse of P in voxel-index space (same formulas as
+    the device preparation kernel); used to count ray samples."""
+    s = np.asarray(spacing_zyx, np.float64)[::-1]
+    o = np.asarray(origin_zyx, np.float64)[::-1]
+    P = np.asarray(P, np.float64)
+    M = P[:, :, :3]
+    Minv = np.linalg.inv(M)
+    C = -np.einsum("nij,nj->ni", Minv, P[:, :, 3])
+    src = (C - o) / s
+    inv_ar = Minv / s[None, :, None]
+    return inv_ar, src
+
+
+def count_samples(cfg, device):
+    """Total ray samples of one forward projection (box [0, N], first sample
+    half a step in, one per step while inside), counted in FP64 on the GPU."""
+    import torch
+    from pyronn_layers import geometry
+    g = geometry.ConeBeam3D(cfg["volume"], (cfg["voxel_mm"],) * 3, cfg["detector"], (cfg["pixel_mm"],) * 2,
+                            cfg["views"], cfg["sid_mm"], cfg["sdd_mm"], step_size=cfg["step_voxels"])
+    inv_ar, src = decompose_np(g.projection_matrices, g.volume_spacing, g.volume_origin)
+    H, W = cfg["detector"]
+    Z, Y, X = cfg["volume"]
+    n_dim = torch.tensor([X, Y, Z], dtype=torch.float64, device=device)
+    vv, uu = torch.meshgrid(torch.arange(H, device=device, dtype=torch.float64),
+                            torch.arange(W, device=device, dtype=torch.float64), indexing="ij")
+    uv1 = torch.stack([uu.flatten(), vv.flatten(), torch.ones_like(uu).flatten()], 0)
+    h = cfg["step_voxels"]
+    total = 0
+    for p in range(cfg["views"]):
+        r = torch.as_tensor(inv_ar[p], device=device) @ uv1
+        r = r / torch.linalg.norm(r, dim=0, keepdim=True)
+        s = torch.as_tensor(src[p], device=device)[:, None]
+        with np.errstate(divide="ignore"):
+            a0 = (0.0 - s) / r
+            a1 = (n_dim[:, None] - s) / r
+        amin = torch.minimum(a0, a1).max(dim=0).values
+        amax = torch.maximum(a0, a1).min(dim=0).values
+        start = amin + 0.5 * h
+        n = torch.nan_to_num(torch.clamp(torch.ceil((amax - start) / h), min=0), nan=0.0, posinf=0.0)
+        total += int(n.sum().item())
+    return total
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks / throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu_index = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--id=%s" % self.gpu_index, "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.rows = []
+        if self.proc is None:
+            return False
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        for row in csv.reader(io.StringIO(out)):
+            if len(row) >= 9:
+                self.rows.append([c.strip() for c in row])
+        return False
+
+    def summary(self):
+        if not getattr(self, "rows", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(self.rows),
+                "power_w_max": max(float(r[3]) for r in self.rows if r[3].replace(".", "").isdigit())
+                if any(r[3].replace(".", "").isdigit() for r in self.rows) else None}
+
+
+def physical_gpu_index(local_rank):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        if local_rank < len(ids):
+            return ids[local_rank]
+    return str(local_rank)
+
+
+# ------------------------------------------------------------------ CPU legs
+
+
+def cpu_sample(cfg, geo, vol_np, sino_np, target_s=8.0, threads=None):
+    """Times the FP64 oracle on a bounded sample and returns
+    (gups, sample description, threads, outputs for the accuracy check)."""
+    import oracle
+    threads = threads or (os.cpu_count() or 1)
+    n_views, n_slices = 1, 2
+    Z = cfg["volume"][0]
+    t0 = time.perf_counter()
+    fwd, _ = oracle.cone_projection3d_views(vol_np, geo.detector_shape, 0, n_views, geo.volume_origin,
+                                            geo.volume_spacing, geo.projection_matrices, geo.step_size,
+                                            nthreads=threads)
+    t_fwd = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    z0 = Z // 2 - n_slices // 2
+    back = oracle.cone_backprojection3d_slab(sino_np, geo.volume_shape, z0, z0 + n_slices, geo.volume_origin,
+                                             geo.volume_spacing, geo.projection_matrices,
+                                             geo.projection_multiplier, nthreads=threads)
+    t_back = time.perf_counter() - t0
+    t_full = t_fwd * cfg["views"] / n_views + t_back * Z / n_slices
+    gups = 2 * updates(cfg) / t_full / 1e9
+    desc = ("forward of %d of %d views + backprojection of %d of %d z-slices, FP64 oracle, scaled to the full step"
+            % (n_views, cfg["views"], n_slices, Z))
+    return gups, desc, threads, dict(fwd=fwd[:n_views], back=back[z0:z0 + n_slices], z0=z0, n_views=n_views,
+                                     n_slices=n_slices, seconds=t_fwd + t_back)
+
+
+def run_reference(args, cfg):
+    """Reference arm: the CPU oracle on bounded samples, rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from pyronn_layers import geometry, phantoms
+    geo = geometry.ConeBeam3D(cfg["volume"], (cfg["voxel_mm"],) * 3, cfg["detector"], (cfg["pixel_mm"],) * 2,
+                              cfg["views"], cfg["sid_mm"], cfg["sdd_mm"], step_size=cfg["step_voxels"])
+    ell = phantoms.random_ellipsoids(shard_seed(2024, 0), [cfg["volume"][i] * cfg["voxel_mm"] for i in (2, 1, 0)],
+                                     n=PHANTOM_ELLIPSOIDS)
+    try:
+        import torch
+        dev = "cuda" if torch.cuda.is_available() else "cpu"
+        vol = phantoms.rasterise_ellipsoids_torch(ell, cfg["volume"], geo.volume_spacing, geo.volume_origin,
+                                                  dev).cpu().numpy()
+    except ImportError:
+        vol = phantoms.rasterise_ellipsoids(ell, cfg["volume"], geo.volume_spacing, geo.volume_origin)
+    rng = np.random.Generator(np.random.PCG64(5))
+    sino = rng.uniform(0, 50, geo.detector_shape).astype(np.float32)
+    times = []
+    for i in range(args.warmup + args.steps):
+        gups, desc, threads, _ = cpu_sample(cfg, geo, vol, sino)
+        if i >= args.warmup:
+            times.append(2 * updates(cfg) / gups / 1e9)
+    t = sum(times)
+    value = 2 * updates(cfg) * args.steps / t / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GUPS", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_block(args, cfg),
+        "cpu_baseline": {"value": value, "unit": "GUPS", "cores": threads, "kind": "port", "sample": desc},
+        "e2e": {"value": value, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def config_block(args, cfg):
+    z, y, x = cfg["volume"]
+    return {"workload": args.workload, "volume": list(cfg["volume"]), "voxel_mm": cfg["voxel_mm"],
+            "views": cfg["views"], "detector_hw": list(cfg["detector"]), "pixel_mm": cfg["pixel_mm"],
+            "sid_mm": cfg["sid_mm"], "sdd_mm": cfg["sdd_mm"], "step_voxels": cfg["step_voxels"],
+            "hardware_interp": bool(args.hardware_interp), "storage": args.storage,
+            "updates_per_op": updates(cfg), "phantom": "%d seeded ellipsoids" % PHANTOM_ELLIPSOIDS,
+            "l2": "inputs larger than L2 (volume %d MB, sinogram %d MB at the storage dtype)"
+                  % (z * y * x * (4 if args.storage == "fp32" else 2) >> 20,
+                     cfg["views"] * cfg["detector"][0] * cfg["detector"][1] * (4 if args.storage == "fp32" else 2)
+                     >> 20),
+            "parallelism": "replicas (one volume per GPU)" if args.gpus > 1 else "single GPU"}
+
+
+# ------------------------------------------------------------------ our arm
+
+
+def run_ours(args, cfg):
+    import torch
+    import torch.distributed as dist
+
+    import pyronn_layers as pl
+    from pyronn_layers import geometry, ops, phantoms
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    dev = torch.device("cuda", local_rank)
+    storage = {"bf16": torch.bfloat16, "fp16": torch.float16, "fp32": torch.float32}[args.storage]
+
+    geo = geometry.ConeBeam3D(cfg["volume"], (cfg["voxel_mm"],) * 3, cfg["detector"], (cfg["pixel_mm"],) * 2,
+                              cfg["views"], cfg["sid_mm"], cfg["sdd_mm"], step_size=cfg["step_voxels"])
+    ell = phantoms.random_ellipsoids(shard_seed(2024, rank),
+                                     [cfg["volume"][i] * cfg["voxel_mm"] for i in (2, 1, 0)], n=PHANTOM_ELLIPSOIDS)
+    vol32 = phantoms.rasterise_ellipsoids_torch(ell, cfg["volume"], geo.volume_spacing, geo.volume_origin, dev)
+    n_proj = cfg["views"]
+    H, W = cfg["detector"]
+    Z, Y, X = cfg["volume"]
+    hw = bool(args.hardware_interp)
+
+    # prepared device geometry and workspaces (what a serving caller keeps resident)
+    gc = ops.GeometryCone(1, dev, *geo.args(), n_proj)
+
+    def make_step(store, out_fwd, out_back):
+        x = vol32.to(store)[None].contiguous()
+        sino = torch.empty((1, n_proj, H, W), dtype=out_fwd, device=dev)
+        back = torch.empty((1, Z, Y, X), dtype=out_back, device=dev)
+        ws_f = torch.empty(pl._capi.workspace_size("pyronn_cone_projection3d", 1, n_proj), dtype=torch.uint8,
+                           device=dev)
+        ws_b = torch.empty(pl._capi.workspace_size("pyronn_cone_backprojection3d", 1, n_proj), dtype=torch.uint8,
+                           device=dev)
+        lib = pl._capi
+        gp = gc.pointers()
+        sf, so, sb = ops.storage_code(store), ops.storage_code(out_fwd), ops.storage_code(out_back)
+        ev = []
+
+        def fwd():
+            lib.call("pyronn_cone_projection3d", x.data_ptr(), sino.data_ptr(), sf, so, int(hw), 1, Z, Y, X, n_proj,
+                     H, W, *gp, 1, ws_f.data_ptr(), ws_f.numel(), torch.cuda.current_stream(dev).cuda_stream)
+
+        def bwd():
+            lib.call("pyronn_cone_backprojection3d", sino.data_ptr(), back.data_ptr(), so, sb, int(hw), 1, n_proj,
+                     H, W, Z, Y, X, *gp, 1, ws_b.data_ptr(), ws_b.numel(), torch.cuda.current_stream(dev).cuda_stream)
+
+        def step(record=False):
+            if record:
+                e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+                e[0].record()
+                fwd()
+                e[1].record()
+                bwd()
+                e[2].record()
+                ev.append(e)
+            else:
+                fwd()
+                bwd()
+
+        return step, ev, x, sino, back
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def timed(step, steps, warmup, record):
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        barrier()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for _ in range(steps):
+            step(record) if record is not None else step()
+        end.record()
+        torch.cuda.synchronize()
+        barrier()
+        ms = start.elapsed_time(end)
+        if world > 1:
+            t = torch.tensor([ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    # ---- the headline configuration (storage dtype in, FP32 volume out)
+    out_fwd = storage
+    step, ev, x, sino, back = make_step(storage, out_fwd, torch.float32)
+    with ClockSampler(physical_gpu_index(local_rank)) as clk:
+        ms = timed(lambda rec=False: step(rec), args.steps, args.warmup, True)
+    clocks = clk.summary()
+    fwd_ms = [a.elapsed_time(b) for a, b, _ in ev]
+    back_ms = [b.elapsed_time(c) for _, b, c in ev]
+    value = 2 * updates(cfg) * world * args.steps / (ms / 1e3) / 1e9
+
+    # ---- the plain FP32 path on the same GPU (same kernels, FP32 storage)
+    fp32_gups = None
+    if storage != torch.float32:
+        step32, _, _, _, _ = make_step(torch.float32, torch.float32, torch.float32)
+        ms32 = timed(lambda rec=False: step32(), args.steps, args.warmup, None)
+        fp32_gups = 2 * updates(cfg) * world * args.steps / (ms32 / 1e3) / 1e9
+        del step32
+        torch.cuda.empty_cache()
+
+    # ---- end to end through the public API: pinned host volume in, volume out
+    host_in = torch.empty((1, Z, Y, X), dtype=storage, pin_memory=True)
+    host_in.copy_(x.cpu())
+    host_out = torch.empty((1, Z, Y, X), dtype=torch.float32, pin_memory=True)
+    args_geo = geo.args()
+
+    def e2e_step(rec=False):
+        xd = host_in.to(dev, non_blocking=True)
+        s = pl.cone_projection3d(xd, geo.detector_shape, *args_geo, hardware_interp=hw)
+        b = pl.cone_backprojection3d(s, geo.volume_shape, *args_geo, hardware_interp=hw, out_dtype=torch.float32)
+        host_out.copy_(b, non_blocking=True)
+
+    e2e_steps = max(2, min(args.steps, 5))
+    e2e_ms = timed(e2e_step, e2e_steps, min(args.warmup, 3), None)
+    e2e_value = 2 * updates(cfg) * world * e2e_steps / (e2e_ms / 1e3) / 1e9
+
+    # ---- roofline of the dominant kernel
+    es = 2 if storage != torch.float32 else 4
+    S = count_samples(cfg, dev)
+    f_ms, b_ms = statistics.mean(fwd_ms), statistics.mean(back_ms)
+    fwd_bytes = S * 8 * es + n_proj * H * W * es
+    back_bytes = updates(cfg) * 4 * es + Z * Y * X * 4
+    peak, peak_kind = measured_peaks()
+    if f_ms >= b_ms:
+        dom, dom_bytes, dom_ms = "cone_fp_kernel (forward)", fwd_bytes, f_ms
+    else:
+        dom, dom_bytes, dom_ms = "cone_bp_kernel (backprojection)", back_bytes, b_ms
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": "%s HBM copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"
+                % peak_kind if peak_kind == "measured" else "fallback 6.65 TB/s",
+                "traffic": args.traffic_bytes,
+                "algorithmic_bytes_per_launch": dom_bytes,
+                "note": "algorithmic bytes = interpolation taps x element size (+ output); frac > 1 means the "
+                        "gathers are served on chip, traffic (ncu dram bytes) is the HBM side"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "GUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "storage": args.storage, "data": "synthetic",
+        "config": config_block(args, cfg),
+        "plain_fp32_value": fp32_gups,
+        "storage_over_fp32": (value / fp32_gups) if fp32_gups else None,
+        "kernels": {"forward_ms": f_ms, "backprojection_ms": b_ms, "ray_samples": S,
+                    "forward_gsamples_per_s": S / (f_ms / 1e3) / 1e9,
+                    "backprojection_gups": updates(cfg) / (b_ms / 1e3) / 1e9},
+        "roofline": roofline,
+        "e2e": {"value": e2e_value, "unit": "GUPS", "h2d_bytes_per_step": host_in.numel() * host_in.element_size(),
+                "d2h_bytes_per_step": host_out.numel() * host_out.element_size(), "steps": e2e_steps},
+        "gpu_launches": 4 * args.steps,
+        "clocks": clocks,
+    }
+
+    # ---- CPU baseline (rank 0, N = 1) and accuracy against the FP64 oracle
+    if world == 1 and not args.no_cpu_baseline:
+        vol_np = vol32.cpu().numpy()[None]
+        sino_np = sino.float().cpu().numpy()
+        gups, desc, threads, outs = cpu_sample(cfg, geo, vol_np, sino_np)
+        line["cpu_baseline"] = {"value": gups, "unit": "GUPS", "cores": threads, "kind": "port", "sample": desc}
+        nv, z0, ns = outs["n_views"], outs["z0"], outs["n_slices"]
+        ours_f = sino[0, :nv].float().cpu().numpy()
+        ours_b = back[0, z0:z0 + ns].float().cpu().numpy()
+
+        def rel(a, b):
+            return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+        line["accuracy"] = {
+            "forward_rel_l2_vs_fp64": rel(ours_f, outs["fwd"]),
+            "backprojection_rel_l2_vs_fp64": rel(ours_b, outs["back"]),
+            "note": "forward: %s storage of the FP32 phantom and of the sinogram vs the FP64 oracle on the FP32 "
+                    "phantom (%d view); backprojection: same sinogram, FP32 volume, %d z-slices" % (args.storage,
+                                                                                                  nv, ns)}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cone512")
+    ap.add_argument("--storage", choices=["bf16", "fp16", "fp32"], default="bf16")
+    ap.add_argument("--hardware-interp", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--traffic-bytes", type=float, default=None,
+                    help="dram bytes per launch of the dominant kernel from an ncu capture")
+    args = ap.parse_args(argv)
+    args.warmup = max(args.warmup, 3)  # at least 3 untimed warm-up steps
+    cfg = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, cfg)
+    else:
+        run_ours(args, cfg)
+
+
+if __name__ == "__main__":
+    main()

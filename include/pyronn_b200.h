@@ -1,0 +1,173 @@
+/*
+ * pyronn_b200.h -- C ABI of the B200-native PYRO-NN-Layers projector operators.
+ *
+ * One entry point per reference operator.  Every entry point
+ *   - takes caller-owned DEVICE buffers for the data (volume / sinogram) and for
+ *     the geometry tensors, exactly the tensors the reference TF op receives
+ *     (the reference op kernels read geometry from device memory too);
+ *   - takes the shapes as host integers (the reference copies its int32 shape
+ *     tensor device->host with a blocking cudaMemcpy inside Compute);
+ *   - launches on the caller's stream and never synchronises it;
+ *   - allocates no device memory for the linear data path: scratch comes from
+ *     a caller-provided workspace whose size the *_workspace_size() query
+ *     returns (the hardware_interp paths keep their CUDA arrays in a
+ *     library-owned, stream-aware cache; see pyronn_release_cached_arrays);
+ *   - returns a pyronn_status_t and never exits the process (the reference
+ *     calls exit() from gpuErrchk, cc/kernels/cone_projector_3D_CudaKernel.cu.cc:32-40).
+ *
+ * Geometry tensors are batch-major: row b of a [geom_batch, ...] tensor holds
+ * the geometry of batch element b, like the reference's flat_outer_dims(index)
+ * rows (e.g. cc/ops/cone_projector_3D_OPKernel.cc:235).  geom_batch may be 1
+ * (one geometry shared by every batch element) or equal to batch.
+ * Vector-valued geometry keeps the reference's [z, y, x] (3D) / [y, x] (2D)
+ * order; ray vectors are (x, y) pairs as the reference kernels read them.
+ *
+ * Storage dtypes: in_dtype and out_dtype (PYRONN_FLOAT32, PYRONN_BFLOAT16,
+ * PYRONN_FLOAT16) give the element type of the data input and of the data
+ * output independently (e.g. BF16 volumes gathered, FP32 sinograms written);
+ * every sum accumulates in FP32 and geometry is always FP32 on input
+ * (prepared in FP64 on the device).
+ */
+#ifndef PYRONN_B200_H
+#define PYRONN_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PYRONN_B200_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define PYRONN_API __attribute__((visibility("default")))
+#else
+#define PYRONN_API
+#endif
+
+typedef enum {
+    PYRONN_FLOAT32 = 0,
+    PYRONN_BFLOAT16 = 1,
+    PYRONN_FLOAT16 = 2
+} pyronn_dtype_t;
+
+typedef enum {
+    PYRONN_SUCCESS = 0,
+    PYRONN_ERROR_INVALID_ARGUMENT = 1,
+    PYRONN_ERROR_UNSUPPORTED = 2,
+    PYRONN_ERROR_WORKSPACE_TOO_SMALL = 3,
+    PYRONN_ERROR_CUDA = 4
+} pyronn_status_t;
+
+/* ABI version of the loaded library (PYRONN_B200_ABI_VERSION). */
+PYRONN_API int pyronn_abi_version(void);
+
+/* Static text for a status code. */
+PYRONN_API const char *pyronn_status_string(int status);
+
+/* Detail of the last failing call on the calling host thread ("" if none). */
+PYRONN_API const char *pyronn_last_error(void);
+
+/* Frees the CUDA arrays the hardware_interp paths cached on the current
+ * device.  Waits for the work that still reads them (device synchronise). */
+PYRONN_API int pyronn_release_cached_arrays(void);
+
+/* ---------------------------------------------------------------------------
+ * ParallelProjection2D
+ *   replaces REGISTER_OP("ParallelProjection2D")  cc/ops/par_projector_2D_OPKernel.cc:30-56
+ *   and Parallel_Projection2D_Kernel_Launcher     cc/kernels/par_projector_2D_CudaKernel.cu.cc:149-178
+ *   volume   [batch, vol_y, vol_x]     -> sinogram [batch, n_proj, det_w]
+ *   volume_origin [g,2], detector_origin [g,1], volume_spacing [g,2],
+ *   detector_spacing [g,1], ray_vectors [g, n_proj, 2]   (g = geom_batch)
+ * ------------------------------------------------------------------------- */
+PYRONN_API int pyronn_parallel_projection2d(const void *volume, void *sinogram, int in_dtype, int out_dtype,
+                                 int batch, int vol_y, int vol_x, int n_proj, int det_w,
+                                 const float *volume_origin, const float *detector_origin,
+                                 const float *volume_spacing, const float *detector_spacing,
+                                 const float *ray_vectors, int geom_batch, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * ParallelBackprojection2D
+ *   replaces REGISTER_OP("ParallelBackprojection2D") cc/ops/par_backprojector_2D_OPKernel.cc:26-51
+ *   and Parallel_Backprojection2D_Kernel_Launcher     cc/kernels/par_backprojector_2D_CudaKernel.cu.cc:77-105
+ *   sinogram [batch, n_proj, det_w]    -> volume [batch, vol_y, vol_x]
+ * ------------------------------------------------------------------------- */
+PYRONN_API int pyronn_parallel_backprojection2d(const void *sinogram, void *volume, int in_dtype, int out_dtype,
+                                     int batch, int n_proj, int det_w, int vol_y, int vol_x,
+                                     const float *volume_origin, const float *detector_origin,
+                                     const float *volume_spacing, const float *detector_spacing,
+                                     const float *ray_vectors, int geom_batch, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * FanProjection2D
+ *   replaces REGISTER_OP("FanProjection2D")  cc/ops/fan_projector_2D_OPKernel.cc:26-53
+ *   and Fan_Projection_Kernel_Launcher       cc/kernels/fan_projector_2D_CudaKernel.cu.cc:165-194
+ *   source_2_isocenter_distance [g,1], source_2_detector_distance [g,1],
+ *   central_ray_vectors [g, n_proj, 2]
+ * ------------------------------------------------------------------------- */
+PYRONN_API int pyronn_fan_projection2d(const void *volume, void *sinogram, int in_dtype, int out_dtype,
+                            int batch, int vol_y, int vol_x, int n_proj, int det_w,
+                            const float *volume_origin, const float *detector_origin,
+                            const float *volume_spacing, const float *detector_spacing,
+                            const float *source_2_isocenter_distance,
+                            const float *source_2_detector_distance,
+                            const float *central_ray_vectors, int geom_batch, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * FanBackprojection2D
+ *   replaces REGISTER_OP("FanBackprojection2D") cc/ops/fan_backprojector_2D_OPKernel.cc:26-53
+ *   and Fan_Backprojection2D_Kernel_Launcher    cc/kernels/fan_backprojector_2D_CudaKernel.cu.cc:83-113
+ * ------------------------------------------------------------------------- */
+PYRONN_API int pyronn_fan_backprojection2d(const void *sinogram, void *volume, int in_dtype, int out_dtype,
+                                int batch, int n_proj, int det_w, int vol_y, int vol_x,
+                                const float *volume_origin, const float *detector_origin,
+                                const float *volume_spacing, const float *detector_spacing,
+                                const float *source_2_isocenter_distance,
+                                const float *source_2_detector_distance,
+                                const float *central_ray_vectors, int geom_batch, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * ConeProjection3D
+ *   replaces REGISTER_OP("ConeProjection3D")       cc/ops/cone_projector_3D_OPKernel.cc:34-60,
+ *   its host DecomposeProjectionMatrices           cc/ops/cone_projector_3D_OPKernel.cc:96-182
+ *   (done here in FP64 on the device, into the workspace),
+ *   Cone_Projection_Kernel_Launcher                cc/kernels/cone_projector_3D_CudaKernel.cu.cc:225-257
+ *   and Cone_Projection_Kernel_Tex_Interp_Launcher cc/kernels/cone_projector_3D_CudaKernel_hardware_interp.cu.cc:199-262
+ *   volume [batch, vol_z, vol_y, vol_x] -> sinogram [batch, n_proj, det_h, det_w]
+ *   volume_origin [g,3], volume_spacing [g,3], projection_matrices [g, n_proj, 3, 4],
+ *   step_size [g,1], projection_multiplier [g,1] (unused by the forward op, as
+ *   in the reference)
+ * ------------------------------------------------------------------------- */
+PYRONN_API size_t pyronn_cone_projection3d_workspace_size(int geom_batch, int n_proj);
+
+PYRONN_API int pyronn_cone_projection3d(const void *volume, void *sinogram, int in_dtype, int out_dtype, int hardware_interp,
+                             int batch, int vol_z, int vol_y, int vol_x,
+                             int n_proj, int det_h, int det_w,
+                             const float *volume_origin, const float *volume_spacing,
+                             const float *projection_matrices, const float *step_size,
+                             const float *projection_multiplier, int geom_batch,
+                             void *workspace, size_t workspace_bytes, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * ConeBackprojection3D
+ *   replaces REGISTER_OP("ConeBackprojection3D")       cc/ops/cone_backprojector_3D_OPKernel.cc:27-53,
+ *   Cone_Backprojection3D_Kernel_Launcher              cc/kernels/cone_backprojector_3D_CudaKernel.cu.cc:121-146
+ *   and Cone_Backprojection3D_Kernel_Tex_Interp_Launcher cc/kernels/cone_backprojector_3D_CudaKernel_hardware_interp.cu.cc:251-307
+ *   sinogram [batch, n_proj, det_h, det_w] -> volume [batch, vol_z, vol_y, vol_x]
+ *   step_size is accepted and unused, as in the reference.
+ * ------------------------------------------------------------------------- */
+PYRONN_API size_t pyronn_cone_backprojection3d_workspace_size(int geom_batch, int n_proj);
+
+PYRONN_API int pyronn_cone_backprojection3d(const void *sinogram, void *volume, int in_dtype, int out_dtype, int hardware_interp,
+                                 int batch, int n_proj, int det_h, int det_w,
+                                 int vol_z, int vol_y, int vol_x,
+                                 const float *volume_origin, const float *volume_spacing,
+                                 const float *projection_matrices, const float *step_size,
+                                 const float *projection_multiplier, int geom_batch,
+                                 void *workspace, size_t workspace_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYRONN_B200_H */

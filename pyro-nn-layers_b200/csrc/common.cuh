@@ -1,0 +1,98 @@
+// common.cuh -- device helpers shared by the projector kernels.
+//
+// Storage types: float, __nv_bfloat16 and __half are loaded through the
+// read-only path and widened to FP32; every sum is FP32.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pyronn {
+
+template <typename T>
+__device__ __forceinline__ float load_as_float(const T *p);
+
+template <>
+__device__ __forceinline__ float load_as_float<float>(const float *p)
+{
+    return __ldg(p);
+}
+
+template <>
+__device__ __forceinline__ float load_as_float<__nv_bfloat16>(const __nv_bfloat16 *p)
+{
+    return __bfloat162float(__ldg(p));
+}
+
+template <>
+__device__ __forceinline__ float load_as_float<__half>(const __half *p)
+{
+    return __half2float(__ldg(p));
+}
+
+template <typename T>
+__device__ __forceinline__ void store_from_float(T *p, float v);
+
+template <>
+__device__ __forceinline__ void store_from_float<float>(float *p, float v)
+{
+    *p = v;
+}
+
+template <>
+__device__ __forceinline__ void store_from_float<__nv_bfloat16>(__nv_bfloat16 *p, float v)
+{
+    *p = __float2bfloat16_rn(v);
+}
+
+template <>
+__device__ __forceinline__ void store_from_float<__half>(__half *p, float v)
+{
+    *p = __float2half_rn(v);
+}
+
+// Linear interpolation in the reference's FMA form,
+// a * (1 - t) + b * t == fma(b, t, fma(a, -t, a))
+// (cone_projector_3D_CudaKernel.cu.cc:74-82 uses the same expression).
+__device__ __forceinline__ float lerp_ref(float a, float b, float t)
+{
+    return __fmaf_rn(b, t, __fmaf_rn(a, -t, a));
+}
+
+template <typename T>
+struct type_tag {
+    using type = T;
+};
+
+// Calls f(type_tag<Tin>{}, type_tag<Tout>{}) for the storage types of the
+// given pyronn_dtype_t codes (0 = float, 1 = bfloat16, 2 = half).
+template <typename F>
+cudaError_t dispatch_dtypes(int in_dtype, int out_dtype, F &&f)
+{
+    auto with_out = [&](auto tin) -> cudaError_t {
+        switch (out_dtype) {
+        case 0: return f(tin, type_tag<float>{});
+        case 1: return f(tin, type_tag<__nv_bfloat16>{});
+        case 2: return f(tin, type_tag<__half>{});
+        default: return cudaErrorInvalidValue;
+        }
+    };
+    switch (in_dtype) {
+    case 0: return with_out(type_tag<float>{});
+    case 1: return with_out(type_tag<__nv_bfloat16>{});
+    case 2: return with_out(type_tag<__half>{});
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+// Approximate reciprocal (one MUFU op, <= 1 ulp).
+__device__ __forceinline__ float fast_rcp(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+}  // namespace pyronn

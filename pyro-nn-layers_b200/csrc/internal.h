@@ -1,0 +1,74 @@
+// internal.h -- launcher interfaces between the C-ABI layer and the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../../include/pyronn_b200.h"
+
+namespace pyronn {
+
+// Per-view cone forward geometry in voxel-index space, built in FP64 on the
+// device from P = [M | p4]: inv_ar = diag(1/spacing) M^-1 (row major) and
+// src = (C - origin) / spacing with C = -M^-1 p4 the camera centre.
+struct ConeFpView {
+    double inv_ar[9];
+    double src[3];
+};
+
+// Per-view cone backprojection matrix in voxel-index space:
+// row r = (P[r,0] sx, P[r,1] sy, P[r,2] sz, P[r,:] . (ox, oy, oz, 1)).
+struct ConeBpView {
+    float4 row[3];
+};
+
+struct Dims2D {
+    int batch, vol_y, vol_x, n_proj, det_w, geom_batch;
+};
+
+struct Geom2D {
+    const float *volume_origin, *detector_origin, *volume_spacing, *detector_spacing;
+    const float *rays, *sid, *sdd;  // sid/sdd null for parallel beam
+};
+
+struct Dims3D {
+    int batch, vol_z, vol_y, vol_x, n_proj, det_h, det_w, geom_batch;
+};
+
+// geometry preparation (geometry.cu)
+cudaError_t launch_cone_fp_prepare(const float *P, const float *spacing, const float *origin, int geom_batch,
+                                   int n_proj, ConeFpView *out, cudaStream_t stream);
+cudaError_t launch_cone_bp_prepare(const float *P, const float *spacing, const float *origin, int geom_batch,
+                                   int n_proj, ConeBpView *out, cudaStream_t stream);
+
+// 2D (proj2d.cu)
+cudaError_t launch_projection2d(const void *volume, void *sinogram, int in_dtype, int out_dtype, bool fan,
+                                const Dims2D &d, const Geom2D &g, cudaStream_t stream);
+cudaError_t launch_backprojection2d(const void *sinogram, void *volume, int in_dtype, int out_dtype, bool fan,
+                                    const Dims2D &d, const Geom2D &g, cudaStream_t stream);
+
+// cone (cone_fp.cu / cone_bp.cu); tex == 0 selects the software path
+cudaError_t launch_cone_fp(const void *volume, void *sinogram, int in_dtype, int out_dtype, const Dims3D &d,
+                           int batch_index, const ConeFpView *views, const float *step, const float *spacing,
+                           cudaTextureObject_t tex, cudaStream_t stream);
+cudaError_t launch_cone_bp(const void *sinogram, void *volume, int in_dtype, int out_dtype, const Dims3D &d,
+                           int batch_index, const ConeBpView *views, const float *mult, cudaTextureObject_t tex,
+                           cudaStream_t stream);
+
+// texture-array cache (texcache.cu)
+struct CachedArray;
+enum ArrayKind { ARRAY_VOLUME_3D = 0, ARRAY_SINOGRAM_LAYERED = 1 };
+// Returns an array of the given kind/extent whose previous users are done
+// (or were on the same stream).  half_texels selects an FP16 texel format.
+cudaError_t array_acquire(int kind, int w, int h, int d, bool half_texels, cudaStream_t stream, CachedArray **out);
+cudaTextureObject_t array_texture(CachedArray *a);
+// Copies one batch element (w*h*d elements of dtype) into the array on stream.
+cudaError_t array_fill(CachedArray *a, const void *src, int dtype, cudaStream_t stream);
+// Marks the array as in use by work already enqueued on stream.
+cudaError_t array_release(CachedArray *a, cudaStream_t stream);
+int array_cache_clear();
+
+size_t dtype_size(int dtype);
+
+}  // namespace pyronn

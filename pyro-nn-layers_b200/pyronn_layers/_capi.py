@@ -1,0 +1,105 @@
+"""ctypes binding of the C ABI in ``include/pyronn_b200.h``.
+
+The library ``libpyronn_b200.so`` sits next to this file (built in-tree by
+``pyro-nn-layers_b200/build.py``).  There is no fallback implementation: if the
+library is missing or fails to load, every op raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+LIB_NAME = "libpyronn_b200.so"
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
+
+ABI_VERSION = 1
+
+FLOAT32 = 0
+BFLOAT16 = 1
+FLOAT16 = 2
+
+SUCCESS = 0
+ERROR_INVALID_ARGUMENT = 1
+ERROR_UNSUPPORTED = 2
+ERROR_WORKSPACE_TOO_SMALL = 3
+ERROR_CUDA = 4
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_SZ = ctypes.c_size_t
+
+# name -> (restype, argtypes); mirrors include/pyronn_b200.h
+PROTOTYPES = {
+    "pyronn_abi_version": (_I, []),
+    "pyronn_status_string": (ctypes.c_char_p, [_I]),
+    "pyronn_last_error": (ctypes.c_char_p, []),
+    "pyronn_release_cached_arrays": (_I, []),
+    "pyronn_parallel_projection2d": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _P]),
+    "pyronn_parallel_backprojection2d": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _P]),
+    "pyronn_fan_projection2d": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
+    "pyronn_fan_backprojection2d": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
+    "pyronn_cone_projection3d_workspace_size": (_SZ, [_I, _I]),
+    "pyronn_cone_projection3d": (
+        _I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _P, _SZ, _P]),
+    "pyronn_cone_backprojection3d_workspace_size": (_SZ, [_I, _I]),
+    "pyronn_cone_backprojection3d": (
+        _I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _P, _SZ, _P]),
+}
+
+
+class PyronnError(RuntimeError):
+    """A non-success status returned by the C ABI."""
+
+    def __init__(self, func, status, detail):
+        self.func = func
+        self.status = status
+        self.detail = detail
+        super().__init__("%s failed: %s (status %d)%s" % (
+            func, _status_name(status), status, (": " + detail) if detail else ""))
+
+
+def _status_name(status):
+    return {
+        SUCCESS: "success",
+        ERROR_INVALID_ARGUMENT: "invalid argument",
+        ERROR_UNSUPPORTED: "unsupported",
+        ERROR_WORKSPACE_TOO_SMALL: "workspace too small",
+        ERROR_CUDA: "CUDA error",
+    }.get(status, "unknown status")
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads (once) and returns the library; raises ImportError if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(
+            "%s not found: build it with `python pyro-nn-layers_b200/build.py` "
+            "(there is no CPU fallback for the projector ops)" % path)
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in PROTOTYPES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    ver = lib.pyronn_abi_version()
+    if ver != ABI_VERSION:
+        raise ImportError("%s has ABI version %d, expected %d" % (path, ver, ABI_VERSION))
+    _lib = lib
+    return lib
+
+
+def call(name: str, *args) -> None:
+    """Calls an entry point and raises PyronnError on a non-success status."""
+    lib = load()
+    status = getattr(lib, name)(*args)
+    if status != SUCCESS:
+        detail = lib.pyronn_last_error().decode("utf-8", "replace")
+        raise PyronnError(name, status, detail)
+
+
+def workspace_size(name: str, geom_batch: int, n_proj: int) -> int:
+    return int(getattr(load(), name + "_workspace_size")(geom_batch, n_proj))

@@ -1,0 +1,95 @@
+"""C ABI surface checks that need no GPU: the library loads, exports every
+symbol include/pyronn_b200.h declares, and rejects bad arguments with a
+status code (no CUDA call happens before these checks)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from pyronn_layers import _capi
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "pyronn_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"PYRONN_API\s+[\w\s\*]+?\b(pyronn_\w+)\s*\(", text)))
+
+
+def test_header_declares_the_six_ops():
+    syms = declared_symbols()
+    for op in ("parallel_projection2d", "parallel_backprojection2d", "fan_projection2d", "fan_backprojection2d",
+               "cone_projection3d", "cone_backprojection3d"):
+        assert "pyronn_" + op in syms
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(_capi.LIB_PATH)
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+    assert set(declared_symbols()) == set(_capi.PROTOTYPES)
+
+
+def test_abi_version_and_status_strings():
+    lib = _capi.load()
+    assert lib.pyronn_abi_version() == _capi.ABI_VERSION
+    assert lib.pyronn_status_string(0) == b"success"
+    assert lib.pyronn_status_string(_capi.ERROR_WORKSPACE_TOO_SMALL) == b"workspace too small"
+    assert lib.pyronn_status_string(99) == b"unknown status"
+
+
+def test_workspace_sizes():
+    lib = _capi.load()
+    fp = lib.pyronn_cone_projection3d_workspace_size(2, 360)
+    bp = lib.pyronn_cone_backprojection3d_workspace_size(2, 360)
+    assert fp >= 2 * 360 * 96 and fp % 256 == 0
+    assert bp >= 2 * 360 * 48 and bp % 256 == 0
+    assert lib.pyronn_cone_projection3d_workspace_size(0, 10) == 0
+
+
+FAKE = 4096  # non-null, never dereferenced: validation fails first
+
+
+@pytest.mark.parametrize("in_dt,out_dt,batch,g,msg", [
+    (7, 0, 1, 1, b"in_dtype"),
+    (0, -1, 1, 1, b"out_dtype"),
+    (0, 0, 0, 1, b"batch"),
+    (0, 0, 2, 3, b"geom_batch"),
+])
+def test_2d_rejects_bad_arguments(in_dt, out_dt, batch, g, msg):
+    lib = _capi.load()
+    st = lib.pyronn_fan_backprojection2d(FAKE, FAKE, in_dt, out_dt, batch, 3, 5, 4, 4, FAKE, FAKE, FAKE, FAKE, FAKE,
+                                         FAKE, FAKE, g, None)
+    assert st == _capi.ERROR_INVALID_ARGUMENT
+    assert msg in lib.pyronn_last_error()
+
+
+def test_null_pointers_and_dims():
+    lib = _capi.load()
+    st = lib.pyronn_parallel_projection2d(None, FAKE, 0, 0, 1, 4, 4, 3, 5, FAKE, FAKE, FAKE, FAKE, FAKE, 1, None)
+    assert st == _capi.ERROR_INVALID_ARGUMENT and b"null data" in lib.pyronn_last_error()
+    st = lib.pyronn_parallel_projection2d(FAKE, FAKE, 0, 0, 1, 4, 4, 3, 5, FAKE, None, FAKE, FAKE, FAKE, 1, None)
+    assert st == _capi.ERROR_INVALID_ARGUMENT and b"null geometry" in lib.pyronn_last_error()
+    st = lib.pyronn_parallel_projection2d(FAKE, FAKE, 0, 0, 1, 4, 0, 3, 5, FAKE, FAKE, FAKE, FAKE, FAKE, 1, None)
+    assert st == _capi.ERROR_INVALID_ARGUMENT and b"positive" in lib.pyronn_last_error()
+
+
+def test_cone_rejects_small_workspace_and_huge_sizes():
+    lib = _capi.load()
+    st = lib.pyronn_cone_backprojection3d(FAKE, FAKE, 0, 0, 0, 1, 8, 8, 8, 4, 4, 4, FAKE, FAKE, FAKE, FAKE, FAKE, 1,
+                                          FAKE, 16, None)
+    assert st == _capi.ERROR_WORKSPACE_TOO_SMALL
+    st = lib.pyronn_cone_projection3d(FAKE, FAKE, 0, 0, 0, 1, 2048, 2048, 2048, 4, 4, 4, FAKE, FAKE, FAKE, FAKE,
+                                      FAKE, 1, FAKE, 1 << 20, None)
+    assert st == _capi.ERROR_UNSUPPORTED and b"2^31" in lib.pyronn_last_error()
+
+
+def test_ops_refuse_cpu_tensors():
+    torch = pytest.importorskip("torch")
+    import pyronn_layers as pl
+    from pyronn_layers import geometry
+    geo = geometry.ConeBeam3D((8, 8, 8), (1, 1, 1), (8, 8), (1, 1), 4, 100, 150)
+    with pytest.raises(ValueError, match="CUDA"):
+        pl.cone_projection3d(torch.zeros(1, 8, 8, 8), geo.detector_shape, *geo.args())

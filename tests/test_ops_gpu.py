@@ -1,0 +1,239 @@
+"""GPU parity of the six ops (all storage dtypes, both interpolation modes)
+against the FP64 oracle and against the reference's own outputs (golden
+fixtures).  Every call goes through the C ABI (libpyronn_b200.so).
+
+Tolerances (relative L2):
+  * FP32 arithmetic vs the FP64 oracle on the same (storage-rounded) input:
+    2e-5 for ray marches (thousands of FP32 sums), 1e-5 for backprojections;
+  * hardware_interp (texture unit, 8-bit interpolation weights) vs exact
+    weights: 5e-3;
+  * 16-bit OUTPUT storage adds its rounding: 4e-3 (bf16), 6e-4 (fp16);
+  * against the reference's outputs: 1e-5 on the software cone paths, 5e-3
+    where the reference used texture weights (all 2D ops, hardware_interp).
+"""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+import pyronn_layers as pl
+from pyronn_layers import _capi, geometry, phantoms
+from conftest import load_golden, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+DTYPES = [torch.float32, torch.bfloat16, torch.float16]
+OUT_TOL = {torch.float32: 0.0, torch.bfloat16: 4e-3, torch.float16: 6e-4}
+
+
+def t(a, dev, dtype=torch.float32):
+    return torch.as_tensor(np.asarray(a)).to(device=dev, dtype=dtype)
+
+
+def rounded(x):
+    return x.float().cpu().numpy()
+
+
+# ------------------------------------------------------------------ 2D
+
+
+def _par_setup(dev, dtype):
+    geo = geometry.ParallelBeam2D((48, 56), (1.0, 0.8), 91, 0.9, 36)
+    vol = np.stack([phantoms.ellipse_phantom_2d((48, 56), (1.0, 0.8), seed=s, n=5)[0] for s in (1, 2)])
+    return geo, t(vol, dev, dtype)
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_parallel_projection_vs_oracle(cuda, dtype):
+    geo, x = _par_setup(cuda, dtype)
+    out = pl.parallel_projection2d(x, geo.detector_shape, *geo.args(), out_dtype=torch.float32)
+    ref = oracle.parallel_projection2d(rounded(x), geo.detector_shape, *geo.args())
+    assert rel_l2(out.cpu().numpy(), ref) < 2e-5
+    out16 = pl.parallel_projection2d(x, geo.detector_shape, *geo.args())
+    assert out16.dtype == dtype
+    assert rel_l2(out16.float().cpu().numpy(), ref) < 2e-5 + OUT_TOL[dtype]
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_parallel_backprojection_vs_oracle(cuda, dtype):
+    geo, _ = _par_setup(cuda, dtype)
+    rng = np.random.Generator(np.random.PCG64(3))
+    p = t(rng.uniform(0, 1, (2,) + geo.detector_shape), cuda, dtype)
+    out = pl.parallel_backprojection2d(p, geo.volume_shape, *geo.args(), out_dtype=torch.float32)
+    ref = oracle.parallel_backprojection2d(rounded(p), geo.volume_shape, *geo.args())
+    assert rel_l2(out.cpu().numpy(), ref) < 1e-5
+
+
+def _fan_setup(dev, dtype):
+    geo = geometry.FanBeam2D((40, 52), (0.5, 0.5), 100, 0.5, 45, 70.0, 110.0)
+    vol = np.stack([phantoms.ellipse_phantom_2d((40, 52), (0.5, 0.5), seed=s, n=5)[0] for s in (4, 5, 6)])
+    return geo, t(vol, dev, dtype)
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_fan_projection_vs_oracle(cuda, dtype):
+    geo, x = _fan_setup(cuda, dtype)
+    out = pl.fan_projection2d(x, geo.detector_shape, *geo.args(), out_dtype=torch.float32)
+    ref = oracle.fan_projection2d(rounded(x), geo.detector_shape, *geo.args())
+    assert rel_l2(out.cpu().numpy(), ref) < 2e-5
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_fan_backprojection_vs_oracle(cuda, dtype):
+    geo, _ = _fan_setup(cuda, dtype)
+    rng = np.random.Generator(np.random.PCG64(9))
+    p = t(rng.uniform(0, 1, (3,) + geo.detector_shape), cuda, dtype)
+    out = pl.fan_backprojection2d(p, geo.volume_shape, *geo.args(), out_dtype=torch.float32)
+    ref = oracle.fan_backprojection2d(rounded(p), geo.volume_shape, *geo.args())
+    assert rel_l2(out.cpu().numpy(), ref) < 1e-5
+
+
+def test_axis_aligned_rays(cuda):
+    """Rays with an exactly zero component skip that slab test
+    (par_projector_2D_CudaKernel.cu.cc:36,48)."""
+    vol, _ = phantoms.ellipse_phantom_2d((32, 32), (1.0, 1.0), seed=11, n=4)
+    rays = np.array([[1, 0], [0, 1], [-1, 0], [0, -1], [0.6, 0.8]], np.float32)
+    args = (geometry.centered_origin((32, 32), (1, 1)), geometry.detector_origin_1d(47, 1.0),
+            np.array([1, 1], np.float32), np.array([1.0], np.float32), rays)
+    out = pl.parallel_projection2d(t(vol[None], cuda), (5, 47), *args)
+    ref = oracle.parallel_projection2d(vol[None], (5, 47), *args)
+    assert rel_l2(out.cpu().numpy(), ref) < 2e-5
+
+
+# ------------------------------------------------------------------ cone
+
+
+def _cone_geo(vol_shape=(20, 24, 28), det=(30, 36), n_proj=16, step=0.5):
+    return geometry.ConeBeam3D(vol_shape, (1.0, 0.9, 1.1), det, (1.2, 1.3), n_proj, 160.0, 260.0,
+                               step_size=step, projection_multiplier=0.8)
+
+
+@pytest.mark.parametrize("hw", [False, True])
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_cone_projection_vs_oracle(cuda, dtype, hw):
+    geo = _cone_geo()
+    vol = np.stack([phantoms.ellipsoid_phantom_3d(geo.volume_shape, geo.volume_spacing, seed=s, n=6)[0]
+                    for s in (1, 2)])
+    x = t(vol, cuda, dtype)
+    out = pl.cone_projection3d(x, geo.detector_shape, *geo.args(), hardware_interp=hw, out_dtype=torch.float32)
+    ref = oracle.cone_projection3d(rounded(x), geo.detector_shape, *geo.args(), hardware_interp=hw)
+    tol = 5e-3 if hw else 2e-5
+    assert rel_l2(out.cpu().numpy(), ref) < tol
+
+
+@pytest.mark.parametrize("hw", [False, True])
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_cone_backprojection_vs_oracle(cuda, dtype, hw):
+    geo = _cone_geo()
+    rng = np.random.Generator(np.random.PCG64(5))
+    p = t(rng.uniform(0, 1, (2,) + geo.detector_shape), cuda, dtype)
+    out = pl.cone_backprojection3d(p, geo.volume_shape, *geo.args(), hardware_interp=hw, out_dtype=torch.float32)
+    ref = oracle.cone_backprojection3d(rounded(p), geo.volume_shape, *geo.args(), hardware_interp=hw)
+    tol = 5e-3 if hw else 1e-5
+    assert rel_l2(out.cpu().numpy(), ref) < tol
+    out16 = pl.cone_backprojection3d(p, geo.volume_shape, *geo.args(), hardware_interp=hw)
+    assert rel_l2(out16.float().cpu().numpy(), ref) < tol + OUT_TOL[dtype]
+
+
+def test_cone_backprojection_edge_taps(cuda):
+    """Detector smaller than the shadow: the software path reads the x == W /
+    y == H taps from the next row / next view (the reference's `>` bounds) and
+    zero past the end of the buffer."""
+    geo = geometry.ConeBeam3D((16, 20, 20), (1.0, 1.0, 1.0), (10, 12), (1.5, 1.5), 7, 150.0, 260.0)
+    rng = np.random.Generator(np.random.PCG64(6))
+    p = rng.uniform(0.5, 1, (1,) + geo.detector_shape).astype(np.float32)
+    out = pl.cone_backprojection3d(t(p, cuda), geo.volume_shape, *geo.args())
+    ref = oracle.cone_backprojection3d(p, geo.volume_shape, *geo.args())
+    assert rel_l2(out.cpu().numpy(), ref) < 1e-5
+    clean = oracle.cone_backprojection3d(p, geo.volume_shape, *geo.args(), hardware_interp=True)
+    assert rel_l2(ref, clean) > 1e-3  # the quirk taps really are exercised
+
+
+def test_cone_batch_geometry_rows(cuda):
+    """Per-batch-element geometry rows vs one shared row."""
+    g1 = _cone_geo()
+    g2 = geometry.ConeBeam3D(g1.volume_shape, (1.0, 1.0, 1.0), (30, 36), (1.2, 1.3), 16, 170.0, 250.0,
+                             step_size=0.6)
+    vol = np.stack([phantoms.ellipsoid_phantom_3d(g1.volume_shape, (1, 1, 1), seed=s, n=5)[0] for s in (7, 8)])
+    stacked = [np.stack([a, b]) for a, b in zip(g1.args(), g2.args())]
+    out = pl.cone_projection3d(t(vol, cuda), g1.detector_shape, *stacked).cpu().numpy()
+    for b, g in enumerate((g1, g2)):
+        single = pl.cone_projection3d(t(vol[b:b + 1], cuda), g.detector_shape, *g.args()).cpu().numpy()
+        np.testing.assert_array_equal(out[b], single[0])
+
+
+# ------------------------------------------------------------ golden (reference outputs)
+
+
+def test_golden_parallel(cuda):
+    g = load_golden("parallel2d")
+    args = (g["volume_origin"], g["detector_origin"], g["volume_spacing"], g["detector_spacing"], g["ray_vectors"])
+    out = pl.parallel_projection2d(t(g["volume"], cuda), g["projection_shape"], *args)
+    assert rel_l2(out.cpu().numpy(), g["sinogram_ref"]) < 5e-3
+    out = pl.parallel_backprojection2d(t(g["sinogram_in"], cuda), g["volume"].shape[1:], *args)
+    assert rel_l2(out.cpu().numpy(), g["volume_ref"]) < 5e-3
+
+
+def test_golden_fan(cuda):
+    g = load_golden("fan2d")
+    args = (g["volume_origin"], g["detector_origin"], g["volume_spacing"], g["detector_spacing"], g["sid"], g["sdd"],
+            g["ray_vectors"])
+    out = pl.fan_projection2d(t(g["volume"], cuda), g["projection_shape"], *args)
+    assert rel_l2(out.cpu().numpy(), g["sinogram_ref"]) < 5e-3
+    out = pl.fan_backprojection2d(t(g["sinogram_in"], cuda), g["volume"].shape[1:], *args)
+    assert rel_l2(out.cpu().numpy(), g["volume_ref"]) < 5e-3
+
+
+@pytest.mark.parametrize("name", ["cone3d", "cone3d_edges"])
+@pytest.mark.parametrize("hw", [0, 1])
+def test_golden_cone(cuda, name, hw):
+    g = load_golden(name)
+    args = (g["volume_origin"], g["volume_spacing"], g["projection_matrices"], g["step_size"],
+            g["projection_multiplier"])
+    tol = 5e-3 if hw else 1e-5
+    out = pl.cone_projection3d(t(g["volume"], cuda), g["projection_shape"], *args, hardware_interp=bool(hw))
+    assert rel_l2(out.cpu().numpy(), g["sinogram_ref_hw%d" % hw]) < tol
+    out = pl.cone_backprojection3d(t(g["sinogram_in"], cuda), g["volume"].shape[1:], *args,
+                                   hardware_interp=bool(hw))
+    assert rel_l2(out.cpu().numpy(), g["volume_ref_hw%d" % hw]) < tol
+
+
+# ------------------------------------------------------------ gradients and errors
+
+
+def test_gradients_are_paired_ops(cuda):
+    geo = _cone_geo()
+    x = torch.rand((1,) + geo.volume_shape, device=cuda, requires_grad=True)
+    y = pl.cone_projection3d(x, geo.detector_shape, *geo.args())
+    gy = torch.rand_like(y)
+    (gx,) = torch.autograd.grad(y, x, gy)
+    bp = pl.cone_backprojection3d(gy, geo.volume_shape, *geo.args())
+    torch.testing.assert_close(gx, bp, rtol=0, atol=0)
+
+    g2 = geometry.FanBeam2D((30, 30), (1, 1), 50, 1.0, 20, 80.0, 120.0)
+    p = torch.rand((2,) + g2.detector_shape, device=cuda, requires_grad=True)
+    v = pl.fan_backprojection2d(p, g2.volume_shape, *g2.args())
+    gv = torch.rand_like(v)
+    (gp,) = torch.autograd.grad(v, p, gv)
+    torch.testing.assert_close(gp, pl.fan_projection2d(gv, g2.detector_shape, *g2.args()), rtol=0, atol=0)
+
+
+def test_invalid_arguments_raise(cuda):
+    geo = _cone_geo()
+    x = torch.rand((1,) + geo.volume_shape, device=cuda)
+    with pytest.raises(ValueError):
+        pl.cone_projection3d(x, (16, 30), *geo.args())
+    with pytest.raises(ValueError):
+        pl.cone_projection3d(x[0], geo.detector_shape, *geo.args())
+    with pytest.raises(TypeError):
+        pl.cone_projection3d(x.double(), geo.detector_shape, *geo.args())
+    # geom_batch that is neither 1 nor batch, straight through the C ABI
+    lib = _capi.load()
+    st = lib.pyronn_parallel_projection2d(x.data_ptr(), x.data_ptr(), 0, 0, 2, 4, 4, 3, 5, 1, 1, 1, 1, 1, 3, None)
+    assert st == _capi.ERROR_INVALID_ARGUMENT
+    assert b"geom_batch" in lib.pyronn_last_error()
+    st = lib.pyronn_cone_projection3d(x.data_ptr(), x.data_ptr(), 0, 0, 0, 1, 4, 4, 4, 3, 5, 5, 1, 1, 1, 1, 1, 1,
+                                      None, 0, None)
+    assert st == _capi.ERROR_WORKSPACE_TOO_SMALL
