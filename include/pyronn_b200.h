@@ -68,6 +68,12 @@ PYRONN_API const char *pyronn_status_string(int status);
 /* Detail of the last failing call on the calling host thread ("" if none). */
 PYRONN_API const char *pyronn_last_error(void);
 
+/* Reads the device error flag a cone call left in its workspace (0 = none,
+ * 1 = a bounded wait for a TMA transfer timed out and the result is invalid).
+ * Synchronises the stream.  No counterpart in the reference (which has no
+ * asynchronous error reporting). */
+PYRONN_API int pyronn_workspace_error(const void *workspace, void *stream, int *device_error);
+
 /* Frees the CUDA arrays the hardware_interp paths cached on the current
  * device.  Waits for the work that still reads them (device synchronise). */
 PYRONN_API int pyronn_release_cached_arrays(void);

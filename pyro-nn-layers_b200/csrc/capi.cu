@@ -60,6 +60,10 @@ size_t align_up(size_t n, size_t a)
     return (n + a - 1) / a * a;
 }
 
+// every cone workspace starts with a header whose first word is the device
+// error flag of the call (pyronn::DeviceError), cleared at the start of the call
+constexpr size_t WS_HEADER = 256;
+
 bool valid_dtype(int dtype)
 {
     return dtype == PYRONN_FLOAT32 || dtype == PYRONN_BFLOAT16 || dtype == PYRONN_FLOAT16;
@@ -245,13 +249,25 @@ int pyronn_fan_backprojection2d(const void *sinogram, void *volume, int in_dtype
 size_t pyronn_cone_projection3d_workspace_size(int geom_batch, int n_proj)
 {
     if (geom_batch <= 0 || n_proj <= 0) return 0;
-    return align_up((size_t)geom_batch * n_proj * sizeof(ConeFpView), 256);
+    return WS_HEADER + align_up((size_t)geom_batch * n_proj * sizeof(ConeFpView), 256);
 }
 
 size_t pyronn_cone_backprojection3d_workspace_size(int geom_batch, int n_proj)
 {
     if (geom_batch <= 0 || n_proj <= 0) return 0;
-    return align_up((size_t)geom_batch * n_proj * sizeof(ConeBpView), 256);
+    return WS_HEADER + align_up((size_t)geom_batch * n_proj * sizeof(ConeBpView), 256);
+}
+
+int pyronn_workspace_error(const void *workspace, void *stream, int *device_error)
+{
+    if (!workspace || !device_error) return fail(PYRONN_ERROR_INVALID_ARGUMENT, "workspace_error: null pointer");
+    unsigned flag = 0;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMemcpyAsync(&flag, workspace, sizeof(flag), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e, "workspace_error");
+    *device_error = (int)flag;
+    return ok();
 }
 
 int pyronn_cone_projection3d(const void *volume, void *sinogram, int in_dtype, int out_dtype, int hardware_interp, int batch, int vol_z,
@@ -276,8 +292,10 @@ int pyronn_cone_projection3d(const void *volume, void *sinogram, int in_dtype, i
         if (st) return st;
     }
     cudaStream_t s = (cudaStream_t)stream;
-    ConeFpView *views = (ConeFpView *)workspace;
-    cudaError_t e = launch_cone_fp_prepare(projection_matrices, volume_spacing, volume_origin, geom_batch, n_proj,
+    ConeFpView *views = (ConeFpView *)((char *)workspace + WS_HEADER);
+    cudaError_t e = cudaMemsetAsync(workspace, 0, WS_HEADER, s);
+    if (e != cudaSuccess) return cuda_fail(e, "cone_projection3d: workspace header");
+    e = launch_cone_fp_prepare(projection_matrices, volume_spacing, volume_origin, geom_batch, n_proj,
                                            views, s);
     if (e != cudaSuccess) return cuda_fail(e, "cone_projection3d: geometry preparation");
     if (!hardware_interp) {
@@ -324,12 +342,17 @@ int pyronn_cone_backprojection3d(const void *sinogram, void *volume, int in_dtyp
         if (st) return st;
     }
     cudaStream_t s = (cudaStream_t)stream;
-    ConeBpView *views = (ConeBpView *)workspace;
-    cudaError_t e = launch_cone_bp_prepare(projection_matrices, volume_spacing, volume_origin, geom_batch, n_proj,
-                                           views, s);
+    ConeBpView *views = (ConeBpView *)((char *)workspace + WS_HEADER);
+    unsigned *err = (unsigned *)workspace;
+    cudaError_t e = cudaMemsetAsync(workspace, 0, WS_HEADER, s);
+    if (e != cudaSuccess) return cuda_fail(e, "cone_backprojection3d: workspace header");
+    e = launch_cone_bp_prepare(projection_matrices, volume_spacing, volume_origin, geom_batch, n_proj, views, s);
     if (e != cudaSuccess) return cuda_fail(e, "cone_backprojection3d: geometry preparation");
     if (!hardware_interp) {
-        e = launch_cone_bp(sinogram, volume, in_dtype, out_dtype, d, -1, views, projection_multiplier, 0, s);
+        if (cone_bp_tma_supported(sinogram, in_dtype, d))
+            e = launch_cone_bp_tma(sinogram, volume, in_dtype, out_dtype, d, views, projection_multiplier, err, s);
+        else
+            e = launch_cone_bp(sinogram, volume, in_dtype, out_dtype, d, -1, views, projection_multiplier, 0, s);
         if (e != cudaSuccess) return cuda_fail(e, name);
         return ok();
     }

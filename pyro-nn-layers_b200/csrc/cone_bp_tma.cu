@@ -1,0 +1,373 @@
+// cone_bp_tma.cu -- voxel-driven cone backprojector with TMA-staged detector
+// tiles (software interpolation, the reference's default hardware_interp=false
+// path, cone_backprojector_3D_CudaKernel.cu.cc:84-118).
+//
+// Block = 256 threads = 32 (x) x 8 (y) voxels, each thread walks 8 voxels
+// along z: a 32 x 8 x 8 voxel tile.  Views are processed in passes of
+// BP_K views.  For every view of a pass one warp projects the 8 tile corners,
+// takes the bounding box of the taps the tile can touch (+1 pixel margin), and
+// one thread issues a 3D TMA load of a BW x BH detector box around it into
+// shared memory; the next pass's boxes load while the current pass computes
+// (two stages, one mbarrier per stage, bounded waits).
+//
+// Exactness: the tap indices and weights are computed exactly as the direct
+// path computes them (floor of u/w, frac), only the texel source differs.  TMA
+// zero-fills out-of-range texels, which equals the reference's semantics for
+// taps x < W and y < H; a (tile, view) whose box reaches column W or row H --
+// where the reference's `>` bounds read the next row / next view -- or does
+// not fit the box, or has a corner at w <= 0, is computed from global memory
+// with the reference's tap rules instead.  A (tile, view) whose taps all lie
+// outside the detector contributes zero and is skipped.
+#include <cuda.h>
+
+#include "common.cuh"
+#include "internal.h"
+#include "tma.cuh"
+
+namespace pyronn {
+
+namespace {
+
+constexpr int TB_X = 32;
+constexpr int TB_Y = 8;
+constexpr int TB_Z = 8;  // voxels per thread along z
+constexpr int BP_K = 4;  // views per pass
+constexpr int BOX_W = 64;
+constexpr int BOX_H = 24;
+constexpr int BOX_ELEMS = BOX_W * BOX_H;
+
+enum ViewMode : int { MODE_SMEM = 0, MODE_GLOBAL = 1, MODE_SKIP = 2 };
+
+struct ViewMeta {
+    float4 row[3];  // voxel-index projection matrix rows
+    float u0, v0;   // box origin (pixels), as floats
+    int iu0, iv0;   // box origin, as ints
+    int mode;
+    int pad[3];
+};
+
+template <typename T>
+__device__ __forceinline__ float smem_to_float(const T *p);
+template <>
+__device__ __forceinline__ float smem_to_float<float>(const float *p)
+{
+    return *p;
+}
+template <>
+__device__ __forceinline__ float smem_to_float<__nv_bfloat16>(const __nv_bfloat16 *p)
+{
+    return __bfloat162float(*p);
+}
+template <>
+__device__ __forceinline__ float smem_to_float<__half>(const __half *p)
+{
+    return __half2float(*p);
+}
+
+// tap rules of interp2D, cone_backprojector_3D_CudaKernel.cu.cc:55-82
+template <typename T>
+__device__ __forceinline__ float interp_global(const T *__restrict__ sino, float u, float v, unsigned view_base, int W,
+                                               int H, unsigned total)
+{
+    const float fu = floorf(u), fv = floorf(v);
+    const float tx = u - fu, ty = v - fv;
+    const float fw = (float)W, fh = (float)H;
+    const bool vx0 = fu >= 0.0f && fu <= fw;
+    const bool vx1 = fu >= -1.0f && fu <= fw - 1.0f;
+    const bool vy0 = fv >= 0.0f && fv <= fh;
+    const bool vy1 = fv >= -1.0f && fv <= fh - 1.0f;
+    const int x0 = __float2int_rz(fu), y0 = __float2int_rz(fv);
+    const unsigned i00 = view_base + (unsigned)y0 * (unsigned)W + (unsigned)x0;
+    const unsigned i01 = i00 + 1u, i10 = i00 + (unsigned)W, i11 = i10 + 1u;
+    const float p00 = (vx0 && vy0 && i00 < total) ? load_as_float(sino + i00) : 0.0f;
+    const float p01 = (vx1 && vy0 && i01 < total) ? load_as_float(sino + i01) : 0.0f;
+    const float p10 = (vx0 && vy1 && i10 < total) ? load_as_float(sino + i10) : 0.0f;
+    const float p11 = (vx1 && vy1 && i11 < total) ? load_as_float(sino + i11) : 0.0f;
+    return lerp_ref(lerp_ref(p00, p01, tx), lerp_ref(p10, p11, tx), ty);
+}
+
+template <typename T>
+struct TmaTraits {
+    static constexpr int ALIGN = 16 / (int)sizeof(T);  // TMA x alignment in elements
+};
+
+// Computes the metadata of one pass (warp 0 only): lane = k * 8 + corner.
+template <typename T>
+__device__ __forceinline__ void pass_meta(ViewMeta *meta, const ConeBpView *__restrict__ pv, int n_first, int n_proj,
+                                          int i0, int j0, int k0, int W, int H)
+{
+    const int lane = threadIdx.x & 31;
+    const int k = lane >> 3, c = lane & 7;
+    const int n = n_first + k;
+    const bool live = n < n_proj;
+    float4 r0 = make_float4(0, 0, 0, 0), r1 = r0, r2 = make_float4(0, 0, 0, 1);
+    if (live) {
+        r0 = __ldg(&pv[n].row[0]);
+        r1 = __ldg(&pv[n].row[1]);
+        r2 = __ldg(&pv[n].row[2]);
+    }
+    const float ci = (float)(i0 + ((c & 1) ? TB_X - 1 : 0));
+    const float cj = (float)(j0 + ((c & 2) ? TB_Y - 1 : 0));
+    const float ck = (float)(k0 + ((c & 4) ? TB_Z - 1 : 0));
+    const float un = fmaf(r0.x, ci, fmaf(r0.y, cj, fmaf(r0.z, ck, r0.w)));
+    const float vn = fmaf(r1.x, ci, fmaf(r1.y, cj, fmaf(r1.z, ck, r1.w)));
+    const float wn = fmaf(r2.x, ci, fmaf(r2.y, cj, fmaf(r2.z, ck, r2.w)));
+    float u = un / wn, v = vn / wn;
+    float umin = u, umax = u, vmin = v, vmax = v, wmin = wn;
+    // a NaN corner makes the view take the global path
+    bool finite = isfinite(u) && isfinite(v);
+#pragma unroll
+    for (int off = 1; off < 8; off <<= 1) {
+        umin = fminf(umin, __shfl_xor_sync(0xffffffffu, umin, off));
+        umax = fmaxf(umax, __shfl_xor_sync(0xffffffffu, umax, off));
+        vmin = fminf(vmin, __shfl_xor_sync(0xffffffffu, vmin, off));
+        vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, off));
+        wmin = fminf(wmin, __shfl_xor_sync(0xffffffffu, wmin, off));
+        finite = __shfl_xor_sync(0xffffffffu, (int)finite, off) && finite;
+    }
+    if (live && c == 0) {
+        ViewMeta m;
+        m.row[0] = r0;
+        m.row[1] = r1;
+        m.row[2] = r2;
+        int mode = MODE_GLOBAL;
+        int iu0 = 0, iv0 = 0;
+        if (finite && wmin > 0.0f && fabsf(umin) < 1.0e6f && fabsf(umax) < 1.0e6f && fabsf(vmin) < 1.0e6f &&
+            fabsf(vmax) < 1.0e6f) {
+            // taps span [floor(u), floor(u) + 1]; one pixel of margin each side
+            const int x_lo = (int)floorf(umin) - 1, x_hi = (int)floorf(umax) + 2;
+            const int y_lo = (int)floorf(vmin) - 1, y_hi = (int)floorf(vmax) + 2;
+            if (x_hi < 0 || y_hi < 0 || x_lo > W || y_lo > H) {
+                mode = MODE_SKIP;  // every tap outside the detector and past the quirk row/column
+            } else {
+                const int a = TmaTraits<T>::ALIGN;
+                iu0 = (x_lo >= 0) ? (x_lo / a) * a : -(((-x_lo) + a - 1) / a) * a;
+                iv0 = y_lo;
+                const bool fits = (x_hi - iu0 + 1 <= BOX_W) && (y_hi - iv0 + 1 <= BOX_H);
+                const bool clear_of_quirk = (x_hi <= W - 1) && (y_hi <= H - 1);
+                if (fits && clear_of_quirk) mode = MODE_SMEM;
+            }
+        }
+        m.u0 = (float)iu0;
+        m.v0 = (float)iv0;
+        m.iu0 = iu0;
+        m.iv0 = iv0;
+        m.mode = mode;
+        meta[k] = m;
+    }
+}
+
+template <typename T, typename Tout>
+__global__ void __launch_bounds__(TB_X *TB_Y)
+    cone_bp_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T *__restrict__ sino, Tout *__restrict__ vol,
+                       const ConeBpView *__restrict__ views, const float *__restrict__ mult, int X, int Y, int Z,
+                       int W, int H, int n_proj, int geom_batch, unsigned *__restrict__ err)
+{
+    extern __shared__ __align__(128) unsigned char dyn_smem[];
+    T(*tiles)[BP_K][BOX_ELEMS] = reinterpret_cast<T(*)[BP_K][BOX_ELEMS]>(dyn_smem);  // [2][BP_K][BOX_ELEMS]
+    __shared__ __align__(16) ViewMeta meta[2][BP_K];
+    __shared__ __align__(8) uint64_t full[2];
+
+    const int tid = threadIdx.y * TB_X + threadIdx.x;
+    const int warp = tid >> 5;
+    const int i0 = blockIdx.x * TB_X, j0 = blockIdx.y * TB_Y;
+    const int zblocks = (Z + TB_Z - 1) / TB_Z;
+    const int k0 = (blockIdx.z % zblocks) * TB_Z;
+    const int b = blockIdx.z / zblocks;
+    const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+    const int g = geom_batch == 1 ? 0 : b;
+    const ConeBpView *pv = views + (size_t)g * n_proj;
+    const T *sino_b = sino + (size_t)b * n_proj * H * W;
+    const unsigned total = (unsigned)n_proj * (unsigned)H * (unsigned)W;
+    const int n_pass = (n_proj + BP_K - 1) / BP_K;
+    constexpr unsigned TILE_BYTES = BOX_ELEMS * sizeof(T);
+
+    if (tid == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        fence_mbar_init();
+    }
+    // issues the TMA loads of pass p into stage s (one thread)
+    auto issue = [&](int p, int s) {
+        int n_fast = 0;
+#pragma unroll
+        for (int k = 0; k < BP_K; ++k) n_fast += (p * BP_K + k < n_proj && meta[s][k].mode == MODE_SMEM);
+        mbar_arrive_expect_tx(&full[s], n_fast * TILE_BYTES);
+#pragma unroll
+        for (int k = 0; k < BP_K; ++k) {
+            const int n = p * BP_K + k;
+            if (n < n_proj && meta[s][k].mode == MODE_SMEM)
+                tma_load_3d(&tiles[s][k][0], &tmap, meta[s][k].iu0, meta[s][k].iv0, b * n_proj + n, &full[s]);
+        }
+    };
+    if (warp == 0) {
+        pass_meta<T>(meta[0], pv, 0, n_proj, i0, j0, k0, W, H);
+        __syncwarp();
+    }
+    __syncthreads();
+    if (tid == 0) issue(0, 0);
+
+    float acc[TB_Z];
+#pragma unroll
+    for (int z = 0; z < TB_Z; ++z) acc[z] = 0.0f;
+    const float fi = (float)i, fj = (float)j, fk = (float)k0;
+    constexpr unsigned MAX_IDX = BOX_ELEMS - BOX_W - 2;
+
+    for (int p = 0; p < n_pass; ++p) {
+        const int cur = p & 1, nxt = cur ^ 1;
+        __syncthreads();  // pass p-1 is done with stage nxt
+        if (warp == 0 && p + 1 < n_pass) {
+            pass_meta<T>(meta[nxt], pv, (p + 1) * BP_K, n_proj, i0, j0, k0, W, H);
+            __syncwarp();
+            if (tid == 0) issue(p + 1, nxt);
+        }
+        mbar_wait_bounded(&full[cur], (p >> 1) & 1, err);
+#pragma unroll 1
+        for (int k = 0; k < BP_K; ++k) {
+            const int n = p * BP_K + k;
+            if (n >= n_proj) break;
+            const ViewMeta &m = meta[cur][k];
+            const int mode = m.mode;
+            if (mode == MODE_SKIP) continue;
+            const float4 r0 = m.row[0], r1 = m.row[1], r2 = m.row[2];
+            const float ub = fmaf(r0.x, fi, fmaf(r0.y, fj, fmaf(r0.z, fk, r0.w)));
+            const float vb = fmaf(r1.x, fi, fmaf(r1.y, fj, fmaf(r1.z, fk, r1.w)));
+            const float wb = fmaf(r2.x, fi, fmaf(r2.y, fj, fmaf(r2.z, fk, r2.w)));
+            if (mode == MODE_SMEM) {
+                const T *tile = &tiles[cur][k][0];
+                const float u0 = m.u0, v0 = m.v0;
+#pragma unroll
+                for (int z = 0; z < TB_Z; ++z) {
+                    const float fz = (float)z;
+                    const float rw = fast_rcp(fmaf(r2.z, fz, wb));
+                    // local box coordinates; the subtraction of an integer is exact
+                    const float lu = fmaf(r0.z, fz, ub) * rw - u0;
+                    const float lv = fmaf(r1.z, fz, vb) * rw - v0;
+                    const float fu = floorf(lu), fv = floorf(lv);
+                    const float tx = lu - fu, ty = lv - fv;
+                    unsigned idx = (unsigned)(__float2int_rz(fv) * BOX_W + __float2int_rz(fu));
+                    idx = min(idx, MAX_IDX);  // memory safety only: the margin keeps idx in range
+                    const float p00 = smem_to_float(tile + idx);
+                    const float p01 = smem_to_float(tile + idx + 1);
+                    const float p10 = smem_to_float(tile + idx + BOX_W);
+                    const float p11 = smem_to_float(tile + idx + BOX_W + 1);
+                    const float val = lerp_ref(lerp_ref(p00, p01, tx), lerp_ref(p10, p11, tx), ty);
+                    acc[z] = fmaf(val * rw, rw, acc[z]);
+                }
+            } else {
+                const unsigned view_base = (unsigned)n * (unsigned)H * (unsigned)W;
+#pragma unroll
+                for (int z = 0; z < TB_Z; ++z) {
+                    const float fz = (float)z;
+                    const float rw = fast_rcp(fmaf(r2.z, fz, wb));
+                    const float uu = fmaf(r0.z, fz, ub) * rw, vv = fmaf(r1.z, fz, vb) * rw;
+                    const float val = interp_global<T>(sino_b, uu, vv, view_base, W, H, total);
+                    acc[z] = fmaf(val * rw, rw, acc[z]);
+                }
+            }
+        }
+    }
+    if (i < X && j < Y) {
+        const float mv = mult[g];
+        Tout *vol_b = vol + (size_t)b * Z * Y * X;
+#pragma unroll
+        for (int z = 0; z < TB_Z; ++z)
+            if (k0 + z < Z) store_from_float(vol_b + ((size_t)(k0 + z) * Y + j) * X + i, acc[z] * mv);
+    }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+template <typename T>
+CUtensorMapDataType tma_type();
+template <>
+CUtensorMapDataType tma_type<float>()
+{
+    return CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+}
+template <>
+CUtensorMapDataType tma_type<__nv_bfloat16>()
+{
+    return CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+}
+template <>
+CUtensorMapDataType tma_type<__half>()
+{
+    return CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+}
+
+template <typename Tin, typename Tout>
+cudaError_t launch_typed(const void *sinogram, void *volume, const Dims3D &d, const ConeBpView *views,
+                         const float *mult, unsigned *err, cudaStream_t stream)
+{
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) return cudaErrorNotSupported;
+    CUtensorMap map;
+    const cuuint64_t dims[3] = {(cuuint64_t)d.det_w, (cuuint64_t)d.det_h, (cuuint64_t)d.n_proj * d.batch};
+    const cuuint64_t strides[2] = {(cuuint64_t)d.det_w * sizeof(Tin), (cuuint64_t)d.det_w * d.det_h * sizeof(Tin)};
+    const cuuint32_t box[3] = {BOX_W, BOX_H, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(&map, tma_type<Tin>(), 3, const_cast<void *>(sinogram), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    const int zblocks = (d.vol_z + TB_Z - 1) / TB_Z;
+    const dim3 block(TB_X, TB_Y, 1);
+    const dim3 grid((d.vol_x + TB_X - 1) / TB_X, (d.vol_y + TB_Y - 1) / TB_Y, zblocks * d.batch);
+    const size_t smem = 2 * BP_K * BOX_ELEMS * sizeof(Tin);
+    static bool attr_set = false;  // per instantiation
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(cone_bp_tma_kernel<Tin, Tout>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    cone_bp_tma_kernel<Tin, Tout><<<grid, block, smem, stream>>>(map, (const Tin *)sinogram, (Tout *)volume, views, mult,
+                                                               d.vol_x, d.vol_y, d.vol_z, d.det_w, d.det_h, d.n_proj,
+                                                               d.geom_batch, err);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+// The TMA path needs 16-byte aligned sinogram rows and base, and a grid that
+// fits one launch; the caller falls back to the direct kernel otherwise.
+bool cone_bp_tma_supported(const void *sinogram, int in_dtype, const Dims3D &d)
+{
+    const size_t e = dtype_size(in_dtype);
+    if (e == 0 || ((uintptr_t)sinogram % 16) != 0) return false;
+    if (((size_t)d.det_w * e) % 16 != 0) return false;
+    const long long zb = (d.vol_z + TB_Z - 1) / TB_Z;
+    if (zb * d.batch > 65535 || (d.vol_y + TB_Y - 1) / TB_Y > 65535) return false;
+    if ((long long)d.n_proj * d.batch >= (1LL << 31)) return false;
+    return encode_fn() != nullptr;
+}
+
+cudaError_t launch_cone_bp_tma(const void *sinogram, void *volume, int in_dtype, int out_dtype, const Dims3D &d,
+                               const ConeBpView *views, const float *mult, unsigned *err, cudaStream_t stream)
+{
+    return dispatch_dtypes(in_dtype, out_dtype, [&](auto tin, auto tout) {
+        using Tin = typename decltype(tin)::type;
+        using Tout = typename decltype(tout)::type;
+        return launch_typed<Tin, Tout>(sinogram, volume, d, views, mult, err, stream);
+    });
+}
+
+}  // namespace pyronn

@@ -56,6 +56,11 @@ cudaError_t launch_cone_bp(const void *sinogram, void *volume, int in_dtype, int
                            int batch_index, const ConeBpView *views, const float *mult, cudaTextureObject_t tex,
                            cudaStream_t stream);
 
+// TMA-staged software backprojector (cone_bp_tma.cu); err = device error flag
+bool cone_bp_tma_supported(const void *sinogram, int in_dtype, const Dims3D &d);
+cudaError_t launch_cone_bp_tma(const void *sinogram, void *volume, int in_dtype, int out_dtype, const Dims3D &d,
+                               const ConeBpView *views, const float *mult, unsigned *err, cudaStream_t stream);
+
 // texture-array cache (texcache.cu)
 struct CachedArray;
 enum ArrayKind { ARRAY_VOLUME_3D = 0, ARRAY_SINOGRAM_LAYERED = 1 };

@@ -34,6 +34,7 @@ PROTOTYPES = {
     "pyronn_status_string": (ctypes.c_char_p, [_I]),
     "pyronn_last_error": (ctypes.c_char_p, []),
     "pyronn_release_cached_arrays": (_I, []),
+    "pyronn_workspace_error": (_I, [_P, _P, _P]),
     "pyronn_parallel_projection2d": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _P]),
     "pyronn_parallel_backprojection2d": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _P]),
     "pyronn_fan_projection2d": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _I, _P]),

@@ -11,6 +11,7 @@ Tolerances (relative L2):
   * against the reference's outputs: 1e-5 on the software cone paths, 5e-3
     where the reference used texture weights (all 2D ops, hardware_interp).
 """
+import ctypes
 import math
 
 import numpy as np
@@ -149,6 +150,43 @@ def test_cone_backprojection_edge_taps(cuda):
     assert rel_l2(out.cpu().numpy(), ref) < 1e-5
     clean = oracle.cone_backprojection3d(p, geo.volume_shape, *geo.args(), hardware_interp=True)
     assert rel_l2(ref, clean) > 1e-3  # the quirk taps really are exercised
+
+
+BP_PATH_GEOMETRIES = {
+    # shadow inside the detector, tiles fit the staging box: TMA-staged tiles
+    "staged": dict(vol=(24, 32, 32), det=(40, 64), px=1.2, sid=400.0, sdd=600.0),
+    # magnification ~3: tile footprints overflow the box, per-view global path
+    "magnified": dict(vol=(24, 40, 44), det=(30, 40), px=1.0, sid=90.0, sdd=200.0),
+    # 37-pixel rows are not 16-byte aligned: the direct-gather kernel
+    "unaligned": dict(vol=(24, 32, 32), det=(40, 37), px=1.2, sid=400.0, sdd=600.0),
+}
+
+
+@pytest.mark.parametrize("case", sorted(BP_PATH_GEOMETRIES))
+@pytest.mark.parametrize("dtype", [torch.float32, torch.bfloat16])
+def test_cone_backprojection_kernel_paths(cuda, dtype, case):
+    c = BP_PATH_GEOMETRIES[case]
+    geo = geometry.ConeBeam3D(c["vol"], (1.0, 1.0, 1.0), c["det"], (c["px"], c["px"]), 12, c["sid"], c["sdd"])
+    rng = np.random.Generator(np.random.PCG64(12))
+    p = t(rng.uniform(0, 1, (2,) + geo.detector_shape), cuda, dtype)
+    out = pl.cone_backprojection3d(p, geo.volume_shape, *geo.args(), out_dtype=torch.float32)
+    ref = oracle.cone_backprojection3d(rounded(p), geo.volume_shape, *geo.args())
+    assert rel_l2(out.cpu().numpy(), ref) < 1e-5
+
+
+def test_workspace_error_flag_clear(cuda):
+    geo = _cone_geo()
+    p = torch.rand((1,) + geo.detector_shape, device=cuda)
+    gc = pl.ops.GeometryCone(1, cuda, *geo.args(), geo.detector_shape[0])
+    ws_bytes = _capi.workspace_size("pyronn_cone_backprojection3d", 1, geo.detector_shape[0])
+    ws = torch.full((ws_bytes,), 7, dtype=torch.uint8, device=cuda)
+    out = torch.empty((1,) + geo.volume_shape, device=cuda)
+    _capi.call("pyronn_cone_backprojection3d", p.data_ptr(), out.data_ptr(), 0, 0, 0, 1, *geo.detector_shape,
+               *geo.volume_shape, *gc.pointers(), 1, ws.data_ptr(), ws_bytes, torch.cuda.current_stream().cuda_stream)
+    flag = ctypes.c_int(-1)
+    _capi.call("pyronn_workspace_error", ws.data_ptr(), torch.cuda.current_stream().cuda_stream,
+               ctypes.byref(flag))
+    assert flag.value == 0
 
 
 def test_cone_batch_geometry_rows(cuda):
