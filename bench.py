@@ -307,10 +307,11 @@ def run_ours(args, cfg):
         x = vol32.to(store)[None].contiguous()
         sino = torch.empty((1, n_proj, H, W), dtype=out_fwd, device=dev)
         back = torch.empty((1, Z, Y, X), dtype=out_back, device=dev)
-        ws_f = torch.empty(pl._capi.workspace_size("pyronn_cone_projection3d", 1, n_proj), dtype=torch.uint8,
-                           device=dev)
-        ws_b = torch.empty(pl._capi.workspace_size("pyronn_cone_backprojection3d", 1, n_proj), dtype=torch.uint8,
-                           device=dev)
+        sf0, so0 = ops.storage_code(store), ops.storage_code(out_fwd)
+        ws_f = torch.empty(pl._capi.workspace_size("pyronn_cone_projection3d", 1, Z, Y, X, n_proj, H, W, sf0,
+                                                   int(hw), 1), dtype=torch.uint8, device=dev)
+        ws_b = torch.empty(pl._capi.workspace_size("pyronn_cone_backprojection3d", 1, n_proj, H, W, Z, Y, X, so0,
+                                                   int(hw), 1), dtype=torch.uint8, device=dev)
         lib = pl._capi
         gp = gc.pointers()
         sf, so, sb = ops.storage_code(store), ops.storage_code(out_fwd), ops.storage_code(out_back)

@@ -9,9 +9,10 @@
  *     tensor device->host with a blocking cudaMemcpy inside Compute);
  *   - launches on the caller's stream and never synchronises it;
  *   - allocates no device memory for the linear data path: scratch comes from
- *     a caller-provided workspace whose size the *_workspace_size() query
- *     returns (the hardware_interp paths keep their CUDA arrays in a
- *     library-owned, stream-aware cache; see pyronn_release_cached_arrays);
+ *     a caller-provided workspace (16-byte aligned) whose size the
+ *     *_workspace_size() query returns (the hardware_interp paths keep their
+ *     CUDA arrays in a library-owned, stream-aware cache; see
+ *     pyronn_release_cached_arrays);
  *   - returns a pyronn_status_t and never exits the process (the reference
  *     calls exit() from gpuErrchk, cc/kernels/cone_projector_3D_CudaKernel.cu.cc:32-40).
  *
@@ -144,7 +145,12 @@ PYRONN_API int pyronn_fan_backprojection2d(const void *sinogram, void *volume, i
  *   step_size [g,1], projection_multiplier [g,1] (unused by the forward op, as
  *   in the reference)
  * ------------------------------------------------------------------------- */
-PYRONN_API size_t pyronn_cone_projection3d_workspace_size(int geom_batch, int n_proj);
+/* Workspace bytes a pyronn_cone_projection3d call with these arguments needs
+ * (prepared geometry; for hardware_interp = 0 also two zero-padded copies of
+ * one volume in the input dtype). */
+PYRONN_API size_t pyronn_cone_projection3d_workspace_size(int batch, int vol_z, int vol_y, int vol_x, int n_proj,
+                                                          int det_h, int det_w, int in_dtype, int hardware_interp,
+                                                          int geom_batch);
 
 PYRONN_API int pyronn_cone_projection3d(const void *volume, void *sinogram, int in_dtype, int out_dtype, int hardware_interp,
                              int batch, int vol_z, int vol_y, int vol_x,
@@ -162,7 +168,10 @@ PYRONN_API int pyronn_cone_projection3d(const void *volume, void *sinogram, int 
  *   sinogram [batch, n_proj, det_h, det_w] -> volume [batch, vol_z, vol_y, vol_x]
  *   step_size is accepted and unused, as in the reference.
  * ------------------------------------------------------------------------- */
-PYRONN_API size_t pyronn_cone_backprojection3d_workspace_size(int geom_batch, int n_proj);
+/* Workspace bytes a pyronn_cone_backprojection3d call with these arguments needs. */
+PYRONN_API size_t pyronn_cone_backprojection3d_workspace_size(int batch, int n_proj, int det_h, int det_w, int vol_z,
+                                                              int vol_y, int vol_x, int in_dtype,
+                                                              int hardware_interp, int geom_batch);
 
 PYRONN_API int pyronn_cone_backprojection3d(const void *sinogram, void *volume, int in_dtype, int out_dtype, int hardware_interp,
                                  int batch, int n_proj, int det_h, int det_w,

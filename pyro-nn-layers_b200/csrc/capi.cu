@@ -246,15 +246,24 @@ int pyronn_fan_backprojection2d(const void *sinogram, void *volume, int in_dtype
     return run_2d(false, true, sinogram, volume, in_dtype, out_dtype, d, g, stream);
 }
 
-size_t pyronn_cone_projection3d_workspace_size(int geom_batch, int n_proj)
+size_t pyronn_cone_projection3d_workspace_size(int batch, int vol_z, int vol_y, int vol_x, int n_proj, int det_h,
+                                               int det_w, int in_dtype, int hardware_interp, int geom_batch)
 {
-    if (geom_batch <= 0 || n_proj <= 0) return 0;
-    return WS_HEADER + align_up((size_t)geom_batch * n_proj * sizeof(ConeFpView), 256);
+    if (geom_batch <= 0 || n_proj <= 0 || batch <= 0 || vol_z <= 0 || vol_y <= 0 || vol_x <= 0 ||
+        !valid_dtype(in_dtype))
+        return 0;
+    size_t n = WS_HEADER + align_up((size_t)geom_batch * n_proj * sizeof(ConeFpView), 256);
+    const Dims3D d{batch, vol_z, vol_y, vol_x, n_proj, det_h, det_w, geom_batch};
+    if (!hardware_interp && cone_fp_padded_supported(d))
+        n += align_up(cone_fp_padded_scratch_bytes(vol_z, vol_y, vol_x, in_dtype), 256);
+    return n;
 }
 
-size_t pyronn_cone_backprojection3d_workspace_size(int geom_batch, int n_proj)
+size_t pyronn_cone_backprojection3d_workspace_size(int batch, int n_proj, int det_h, int det_w, int vol_z, int vol_y,
+                                                   int vol_x, int in_dtype, int hardware_interp, int geom_batch)
 {
-    if (geom_batch <= 0 || n_proj <= 0) return 0;
+    (void)batch, (void)det_h, (void)det_w, (void)vol_z, (void)vol_y, (void)vol_x, (void)hardware_interp;
+    if (geom_batch <= 0 || n_proj <= 0 || !valid_dtype(in_dtype)) return 0;
     return WS_HEADER + align_up((size_t)geom_batch * n_proj * sizeof(ConeBpView), 256);
 }
 
@@ -281,7 +290,8 @@ int pyronn_cone_projection3d(const void *volume, void *sinogram, int in_dtype, i
     int st = check_cone(name, volume, sinogram, in_dtype, out_dtype, d, volume_origin, volume_spacing, projection_matrices,
                         step_size, projection_multiplier);
     if (st) return st;
-    const size_t need = pyronn_cone_projection3d_workspace_size(geom_batch, n_proj);
+    const size_t need = pyronn_cone_projection3d_workspace_size(batch, vol_z, vol_y, vol_x, n_proj, det_h, det_w,
+                                                                in_dtype, hardware_interp, geom_batch);
     if (!workspace || workspace_bytes < need)
         return fail(PYRONN_ERROR_WORKSPACE_TOO_SMALL, "%s: workspace of %zu bytes needed, %zu given", name, need,
                     workspace ? workspace_bytes : (size_t)0);
@@ -299,7 +309,14 @@ int pyronn_cone_projection3d(const void *volume, void *sinogram, int in_dtype, i
                                            views, s);
     if (e != cudaSuccess) return cuda_fail(e, "cone_projection3d: geometry preparation");
     if (!hardware_interp) {
-        e = launch_cone_fp(volume, sinogram, in_dtype, out_dtype, d, -1, views, step_size, volume_spacing, 0, s);
+        if (cone_fp_padded_supported(d)) {
+            void *scratch = (char *)workspace + WS_HEADER +
+                            align_up((size_t)geom_batch * n_proj * sizeof(ConeFpView), 256);
+            e = launch_cone_fp_padded(volume, sinogram, in_dtype, out_dtype, d, views, step_size, volume_spacing,
+                                      scratch, s);
+        } else {
+            e = launch_cone_fp(volume, sinogram, in_dtype, out_dtype, d, -1, views, step_size, volume_spacing, 0, s);
+        }
         if (e != cudaSuccess) return cuda_fail(e, name);
         return ok();
     }
@@ -331,7 +348,8 @@ int pyronn_cone_backprojection3d(const void *sinogram, void *volume, int in_dtyp
     int st = check_cone(name, sinogram, volume, in_dtype, out_dtype, d, volume_origin, volume_spacing, projection_matrices,
                         step_size, projection_multiplier);
     if (st) return st;
-    const size_t need = pyronn_cone_backprojection3d_workspace_size(geom_batch, n_proj);
+    const size_t need = pyronn_cone_backprojection3d_workspace_size(batch, n_proj, det_h, det_w, vol_z, vol_y, vol_x,
+                                                                    in_dtype, hardware_interp, geom_batch);
     if (!workspace || workspace_bytes < need)
         return fail(PYRONN_ERROR_WORKSPACE_TOO_SMALL, "%s: workspace of %zu bytes needed, %zu given", name, need,
                     workspace ? workspace_bytes : (size_t)0);

@@ -56,6 +56,13 @@ cudaError_t launch_cone_bp(const void *sinogram, void *volume, int in_dtype, int
                            int batch_index, const ConeBpView *views, const float *mult, cudaTextureObject_t tex,
                            cudaStream_t stream);
 
+// software forward projector over padded, view-oriented copies (cone_fp_padded.cu)
+size_t cone_fp_padded_scratch_bytes(int vol_z, int vol_y, int vol_x, int in_dtype);
+bool cone_fp_padded_supported(const Dims3D &d);
+cudaError_t launch_cone_fp_padded(const void *volume, void *sinogram, int in_dtype, int out_dtype, const Dims3D &d,
+                                  const ConeFpView *views, const float *step, const float *spacing, void *scratch,
+                                  cudaStream_t stream);
+
 // TMA-staged software backprojector (cone_bp_tma.cu); err = device error flag
 bool cone_bp_tma_supported(const void *sinogram, int in_dtype, const Dims3D &d);
 cudaError_t launch_cone_bp_tma(const void *sinogram, void *volume, int in_dtype, int out_dtype, const Dims3D &d,

@@ -39,10 +39,10 @@ PROTOTYPES = {
     "pyronn_parallel_backprojection2d": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _P]),
     "pyronn_fan_projection2d": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
     "pyronn_fan_backprojection2d": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
-    "pyronn_cone_projection3d_workspace_size": (_SZ, [_I, _I]),
+    "pyronn_cone_projection3d_workspace_size": (_SZ, [_I] * 10),
     "pyronn_cone_projection3d": (
         _I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _P, _SZ, _P]),
-    "pyronn_cone_backprojection3d_workspace_size": (_SZ, [_I, _I]),
+    "pyronn_cone_backprojection3d_workspace_size": (_SZ, [_I] * 10),
     "pyronn_cone_backprojection3d": (
         _I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _P, _SZ, _P]),
 }
@@ -102,5 +102,6 @@ def call(name: str, *args) -> None:
         raise PyronnError(name, status, detail)
 
 
-def workspace_size(name: str, geom_batch: int, n_proj: int) -> int:
-    return int(getattr(load(), name + "_workspace_size")(geom_batch, n_proj))
+def workspace_size(name: str, *args: int) -> int:
+    """Workspace bytes of a cone entry point; args as the C query takes them."""
+    return int(getattr(load(), name + "_workspace_size")(*args))

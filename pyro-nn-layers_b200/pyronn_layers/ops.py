@@ -200,13 +200,15 @@ def _run_cone(forward: bool, x: torch.Tensor, out_dims, geo: GeometryCone, hardw
         out = torch.empty((batch, n_proj, det_h, det_w), dtype=od, device=dev)
         fn = "pyronn_cone_projection3d"
         dims = [batch, vol_z, vol_y, vol_x, n_proj, det_h, det_w]
+        ws_args = dims + [storage_code(x.dtype), int(bool(hardware_interp)), geo.g]
     else:
         n_proj, det_h, det_w = x.shape[1:]
         vol_z, vol_y, vol_x = out_dims
         out = torch.empty((batch, vol_z, vol_y, vol_x), dtype=od, device=dev)
         fn = "pyronn_cone_backprojection3d"
         dims = [batch, n_proj, det_h, det_w, vol_z, vol_y, vol_x]
-    ws_bytes = _capi.workspace_size(fn, geo.g, n_proj)
+        ws_args = dims + [storage_code(x.dtype), int(bool(hardware_interp)), geo.g]
+    ws_bytes = _capi.workspace_size(fn, *ws_args)
     if workspace is None or workspace.numel() < ws_bytes:
         workspace = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
     with torch.cuda.device(dev):

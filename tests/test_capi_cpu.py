@@ -42,11 +42,20 @@ def test_abi_version_and_status_strings():
 
 def test_workspace_sizes():
     lib = _capi.load()
-    fp = lib.pyronn_cone_projection3d_workspace_size(2, 360)
-    bp = lib.pyronn_cone_backprojection3d_workspace_size(2, 360)
-    assert fp >= 2 * 360 * 96 and fp % 256 == 0
-    assert bp >= 2 * 360 * 48 and bp % 256 == 0
-    assert lib.pyronn_cone_projection3d_workspace_size(0, 10) == 0
+    # batch, vol z/y/x, views, det h/w, in_dtype, hardware_interp, geom_batch
+    fp = lib.pyronn_cone_projection3d_workspace_size(2, 64, 64, 64, 360, 100, 120, 0, 0, 2)
+    fp_hw = lib.pyronn_cone_projection3d_workspace_size(2, 64, 64, 64, 360, 100, 120, 0, 1, 2)
+    fp16 = lib.pyronn_cone_projection3d_workspace_size(2, 64, 64, 64, 360, 100, 120, 1, 0, 2)
+    bp = lib.pyronn_cone_backprojection3d_workspace_size(2, 360, 100, 120, 64, 64, 64, 0, 0, 2)
+    assert fp_hw >= 256 + 2 * 360 * 96 and fp_hw % 256 == 0
+    # two zero-padded copies of one volume for the software forward path
+    def align(n):
+        return (n + 255) // 256 * 256
+    assert fp - fp_hw == align(2 * 67 ** 3 * 4)
+    assert fp16 - fp_hw == align(2 * 67 ** 3 * 2)
+    assert bp >= 256 + 2 * 360 * 48 and bp % 256 == 0
+    assert lib.pyronn_cone_projection3d_workspace_size(0, 8, 8, 8, 10, 4, 4, 0, 0, 1) == 0
+    assert lib.pyronn_cone_projection3d_workspace_size(1, 8, 8, 8, 10, 4, 4, 9, 0, 1) == 0
 
 
 FAKE = 4096  # non-null, never dereferenced: validation fails first

@@ -178,7 +178,7 @@ def test_workspace_error_flag_clear(cuda):
     geo = _cone_geo()
     p = torch.rand((1,) + geo.detector_shape, device=cuda)
     gc = pl.ops.GeometryCone(1, cuda, *geo.args(), geo.detector_shape[0])
-    ws_bytes = _capi.workspace_size("pyronn_cone_backprojection3d", 1, geo.detector_shape[0])
+    ws_bytes = _capi.workspace_size("pyronn_cone_backprojection3d", 1, *geo.detector_shape, *geo.volume_shape, 0, 0, 1)
     ws = torch.full((ws_bytes,), 7, dtype=torch.uint8, device=cuda)
     out = torch.empty((1,) + geo.volume_shape, device=cuda)
     _capi.call("pyronn_cone_backprojection3d", p.data_ptr(), out.data_ptr(), 0, 0, 0, 1, *geo.detector_shape,
