@@ -181,6 +181,25 @@ PYRONN_API int pyronn_cone_backprojection3d(const void *sinogram, void *volume, 
                                  const float *projection_multiplier, int geom_batch,
                                  void *workspace, size_t workspace_bytes, void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Matched cone backprojection: the exact transpose of the software-interpolation
+ * ConeProjection3D (ray-driven scatter with the projector's own samples and
+ * weights, FP32 atomics).  No counterpart in the reference, whose voxel-driven
+ * ConeBackprojection3D is not the transpose of its projector; this is the
+ * adjoint a dot-product test <A x, y> = <x, A^T y> holds for (exact for every
+ * ray whose line integral is > 0, e.g. any non-negative volume).
+ *   sinogram [batch, n_proj, det_h, det_w] (in_dtype) -> volume [batch, vol_z,
+ *   vol_y, vol_x] FP32 (overwritten); projection_multiplier is not applied.
+ * ------------------------------------------------------------------------- */
+PYRONN_API size_t pyronn_cone_backprojection3d_matched_workspace_size(int geom_batch, int n_proj);
+
+PYRONN_API int pyronn_cone_backprojection3d_matched(const void *sinogram, float *volume, int in_dtype, int batch,
+                                                    int n_proj, int det_h, int det_w, int vol_z, int vol_y,
+                                                    int vol_x, const float *volume_origin,
+                                                    const float *volume_spacing, const float *projection_matrices,
+                                                    const float *step_size, int geom_batch, void *workspace,
+                                                    size_t workspace_bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -97,9 +97,11 @@ def lib():
         L.oracle_cone_decompose.argtypes = [P, P, P, I, P, P]
         L.oracle_cone_backprojection3d_slab.argtypes = [P, P, I, I, I, I, I, I, I, I, I, P, P, P, P, I]
         L.oracle_cone_projection3d_views.argtypes = [P, P, I, I, I, I, I, I, I, I, I, P, P, P, P, I, P]
+        L.oracle_cone_backprojection3d_matched.argtypes = [P, P, I, I, I, I, I, I, I, P, P, P, P, I]
         for f in ("oracle_parallel_projection2d", "oracle_fan_projection2d", "oracle_parallel_backprojection2d",
                   "oracle_fan_backprojection2d", "oracle_cone_projection3d", "oracle_cone_backprojection3d",
-                  "oracle_cone_decompose", "oracle_cone_backprojection3d_slab", "oracle_cone_projection3d_views"):
+                  "oracle_cone_decompose", "oracle_cone_backprojection3d_slab", "oracle_cone_projection3d_views",
+                  "oracle_cone_backprojection3d_matched"):
             getattr(L, f).restype = None
         _lib = L
     return _lib
@@ -258,3 +260,18 @@ def cone_projection3d_views(volume, projection_shape, p_begin, p_end, volume_ori
         _ptr(_f32(volume_origin)), _ptr(_f32(volume_spacing)), _ptr(_f32(projection_matrices)),
         _ptr(_f32(np.atleast_1d(step_size))), nthreads or default_threads(), _ptr(cnt))
     return out, cnt
+
+
+def cone_backprojection3d_matched(sinogram, volume_shape, volume_origin, volume_spacing, projection_matrices,
+                                  step_size, projection_multiplier=None):
+    """Exact transpose of the linear software forward projector (FP64)."""
+    sino = _f32(sinogram)
+    B, n_proj, H, W = sino.shape
+    Z, Y, X = (int(v) for v in volume_shape)
+    g = _geom_batch(B, (_f32(volume_origin), 3), (_f32(projection_matrices), n_proj * 12))
+    args = [_rows(volume_origin, g, 3), _rows(volume_spacing, g, 3), _rows(projection_matrices, g, 12 * n_proj),
+            _rows(step_size, g, 1)]
+    out = np.zeros((B, Z, Y, X), dtype=np.float64)
+    lib().oracle_cone_backprojection3d_matched(_ptr(sino), _ptr(out), B, n_proj, H, W, Z, Y, X,
+                                               *[_ptr(a) for a in args], g)
+    return out

@@ -611,3 +611,90 @@ void oracle_cone_projection3d_views(const float *vol, double *sino, int hardware
     free(invAR);
     free(src);
 }
+
+/* ------------------------------------------- matched (transpose) backprojection */
+
+static void scatter_trilinear(double *vol, long X, long Y, long Z, double x, double y, double z, double val)
+{
+    double xf = floor(x), yf = floor(y), zf = floor(z);
+    double fx = x - xf, fy = y - yf, fz = z - zf;
+    long x0 = (long)xf, y0 = (long)yf, z0 = (long)zf;
+    double wx[2] = {1.0 - fx, fx}, wy[2] = {1.0 - fy, fy}, wz[2] = {1.0 - fz, fz};
+    for (int dz = 0; dz < 2; ++dz)
+        for (int dy = 0; dy < 2; ++dy)
+            for (int dx = 0; dx < 2; ++dx) {
+                long xx = x0 + dx, yy = y0 + dy, zz = z0 + dz;
+                if (xx < 0 || xx >= X || yy < 0 || yy >= Y || zz < 0 || zz >= Z) continue;
+                vol[(zz * Y + yy) * X + xx] += val * wz[dz] * wy[dy] * wx[dx];
+            }
+}
+
+/* Transpose of the software forward projector with the end correction always
+ * applied (the linear form of cone_projector_3D_CudaKernel.cu.cc:135-179):
+ * every sample scatters sino * (its trapezoid weight) * |ray (.) spacing|
+ * into its 8 trilinear taps.  Single-threaded per batch element (test sizes). */
+void oracle_cone_backprojection3d_matched(const float *sino, double *vol, int batch, int n_proj, int H, int W, int Z,
+                                          int Y, int X, const float *vol_origin, const float *vol_spacing,
+                                          const float *P, const float *step, int geom_batch)
+{
+    double *invAR = (double *)malloc(sizeof(double) * 9 * (size_t)geom_batch * n_proj);
+    double *src = (double *)malloc(sizeof(double) * 3 * (size_t)geom_batch * n_proj);
+    for (int g = 0; g < geom_batch; ++g)
+        oracle_cone_decompose(P + (size_t)g * n_proj * 12, vol_spacing + 3 * g, vol_origin + 3 * g, n_proj,
+                              invAR + (size_t)g * n_proj * 9, src + (size_t)g * n_proj * 3);
+    long N[3] = {X, Y, Z};
+    memset(vol, 0, sizeof(double) * (size_t)batch * Z * Y * X);
+    for (int b = 0; b < batch; ++b) {
+        int gb = geom_batch == 1 ? 0 : b;
+        double sp[3] = {vol_spacing[gb * 3 + 2], vol_spacing[gb * 3 + 1], vol_spacing[gb * 3 + 0]};
+        float h = step[gb];
+        double *vb = vol + (size_t)b * Z * Y * X;
+        for (int p = 0; p < n_proj; ++p) {
+            const double *M = invAR + ((size_t)gb * n_proj + p) * 9;
+            const double *S = src + ((size_t)gb * n_proj + p) * 3;
+            for (int v = 0; v < H; ++v)
+                for (int u = 0; u < W; ++u) {
+                    double yv = sino[(((size_t)b * n_proj + p) * H + v) * W + u];
+                    if (yv == 0.0) continue;
+                    double r[3];
+                    for (int k = 0; k < 3; ++k) r[k] = M[3 * k + 2] + v * M[3 * k + 1] + u * M[3 * k + 0];
+                    double len = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+                    for (int k = 0; k < 3; ++k) r[k] /= len;
+                    double min_a = 0.0, max_a = INFINITY;
+                    for (int k = 0; k < 3; ++k)
+                        if (r[k] != 0.0) {
+                            double rc = 1.0 / r[k], a0 = (0.0 - S[k]) * rc, a1 = ((double)N[k] - S[k]) * rc;
+                            if (k == 0) {
+                                min_a = fmin(a0, a1);
+                                max_a = fmax(a0, a1);
+                            } else {
+                                min_a = fmax(min_a, fmin(a0, a1));
+                                max_a = fmin(max_a, fmax(a0, a1));
+                            }
+                        }
+                    float a = (float)min_a;
+                    a += h * 0.5f;
+                    float amax = (float)max_a;
+                    if (!(a < amax)) continue;
+                    double scale = yv * sqrt((r[0] * sp[0]) * (r[0] * sp[0]) + (r[1] * sp[1]) * (r[1] * sp[1]) +
+                                             (r[2] * sp[2]) * (r[2] * sp[2]));
+                    double held = 0.5 * (double)h, pt[3];
+                    for (int k = 0; k < 3; ++k) pt[k] = S[k] + (double)a * r[k];
+                    a += h;
+                    while (a < amax) {
+                        scatter_trilinear(vb, X, Y, Z, pt[0], pt[1], pt[2], held * scale);
+                        for (int k = 0; k < 3; ++k) pt[k] = S[k] + (double)a * r[k];
+                        held = (double)h;
+                        a += h;
+                    }
+                    a -= h;
+                    double last = (double)amax - (double)a;
+                    scatter_trilinear(vb, X, Y, Z, pt[0], pt[1], pt[2], (held - 0.5 * (double)h + 0.5 * last) * scale);
+                    for (int k = 0; k < 3; ++k) pt[k] = S[k] + (double)amax * r[k];
+                    scatter_trilinear(vb, X, Y, Z, pt[0], pt[1], pt[2], 0.5 * last * scale);
+                }
+        }
+    }
+    free(invAR);
+    free(src);
+}

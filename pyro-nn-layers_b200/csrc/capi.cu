@@ -390,4 +390,41 @@ int pyronn_cone_backprojection3d(const void *sinogram, void *volume, int in_dtyp
     return ok();
 }
 
+size_t pyronn_cone_backprojection3d_matched_workspace_size(int geom_batch, int n_proj)
+{
+    if (geom_batch <= 0 || n_proj <= 0) return 0;
+    return WS_HEADER + align_up((size_t)geom_batch * n_proj * sizeof(ConeFpView), 256);
+}
+
+int pyronn_cone_backprojection3d_matched(const void *sinogram, float *volume, int in_dtype, int batch, int n_proj,
+                                         int det_h, int det_w, int vol_z, int vol_y, int vol_x,
+                                         const float *volume_origin, const float *volume_spacing,
+                                         const float *projection_matrices, const float *step_size, int geom_batch,
+                                         void *workspace, size_t workspace_bytes, void *stream)
+{
+    const char *name = "cone_backprojection3d_matched";
+    const Dims3D d{batch, vol_z, vol_y, vol_x, n_proj, det_h, det_w, geom_batch};
+    // the step is the only scalar the scatter reads; pass it as the multiplier
+    // slot too so the shared checks see a non-null pointer
+    int st = check_cone(name, sinogram, volume, in_dtype, PYRONN_FLOAT32, d, volume_origin, volume_spacing,
+                        projection_matrices, step_size, step_size);
+    if (st) return st;
+    if ((long long)n_proj * batch > 65535)
+        return fail(PYRONN_ERROR_UNSUPPORTED, "%s: views x batch above 65535", name);
+    const size_t need = pyronn_cone_backprojection3d_matched_workspace_size(geom_batch, n_proj);
+    if (!workspace || workspace_bytes < need)
+        return fail(PYRONN_ERROR_WORKSPACE_TOO_SMALL, "%s: workspace of %zu bytes needed, %zu given", name, need,
+                    workspace ? workspace_bytes : (size_t)0);
+    if (((uintptr_t)workspace) % 16 != 0)
+        return fail(PYRONN_ERROR_INVALID_ARGUMENT, "%s: workspace must be 16-byte aligned", name);
+    cudaStream_t s = (cudaStream_t)stream;
+    ConeFpView *views = (ConeFpView *)((char *)workspace + WS_HEADER);
+    cudaError_t e = cudaMemsetAsync(workspace, 0, WS_HEADER, s);
+    if (e == cudaSuccess)
+        e = launch_cone_fp_prepare(projection_matrices, volume_spacing, volume_origin, geom_batch, n_proj, views, s);
+    if (e == cudaSuccess) e = launch_cone_scatter(sinogram, volume, in_dtype, d, views, step_size, volume_spacing, s);
+    if (e != cudaSuccess) return cuda_fail(e, name);
+    return ok();
+}
+
 }  // extern "C"

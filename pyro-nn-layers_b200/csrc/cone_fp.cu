@@ -16,6 +16,7 @@
 #include <math_constants.h>
 
 #include "common.cuh"
+#include "cone_ray.cuh"
 #include "internal.h"
 
 namespace pyronn {
@@ -78,86 +79,11 @@ __global__ void __launch_bounds__(FP_BLOCK_X *FP_BLOCK_Y)
     const int b = batch_begin + blockIdx.z / n_proj;
     if (u >= W || v >= H) return;
     const int g = geom_batch == 1 ? 0 : b;
-    const ConeFpView &view = views[(size_t)g * n_proj + p];
-
-    // ray direction in voxel-index space, cone_projector_3D_CudaKernel.cu.cc:200-205 (FP64 here)
-    double r[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-        r[k] = view.inv_ar[3 * k + 2] + (double)v * view.inv_ar[3 * k + 1] + (double)u * view.inv_ar[3 * k + 0];
-    const double inv_len = 1.0 / sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) r[k] *= inv_len;
-    const double s[3] = {view.src[0], view.src[1], view.src[2]};
-
-    // box entry/exit, :96-132 (software) or hardware_interp.cu.cc:51-86, in FP64
-    const double lo = HW ? -0.5 : 0.0;
-    const double n_dim[3] = {(double)X, (double)Y, (double)Z};
-    double amin = 0.0, amax = CUDART_INF;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        if (r[k] != 0.0) {
-            const double rc = 1.0 / r[k];
-            const double a0 = (lo - s[k]) * rc;
-            const double a1 = (n_dim[k] + lo - s[k]) * rc;
-            if (k == 0) {
-                amin = fmin(a0, a1);
-                amax = fmax(a0, a1);
-            } else {
-                amin = fmax(amin, fmin(a0, a1));
-                amax = fmin(amax, fmax(a0, a1));
-            }
-        }
-    }
-
     const float step = step_ptr[g];
-    const float dx = (float)r[0], dy = (float)r[1], dz = (float)r[2];
-    const float sx = (float)s[0], sy = (float)s[1], sz = (float)s[2];
-    float pixel = 0.0f;
-    if (step > 0.0f && step < CUDART_INF_F && amin < amax) {
-        const Sampler<T, HW> sample{vol + (size_t)b * X * Y * Z, tex, X, Y, Z};
-        float a = (float)amin;
-        a += step * 0.5f;
-        const float am = (float)amax;
-        // upper bound on the number of samples: the march stops even where a
-        // float alpha stagnates (the reference would spin forever there)
-        const double bound = ((double)am - (double)a) / (double)step + 4.0;
-        const int max_iter = bound > 1.0e8 ? 100000000 : (int)bound;
-        float px = 0.0f, py = 0.0f, pz = 0.0f;
-        int iter = 0;
-        if (a < am) {
-            px = fmaf(a, dx, sx);
-            py = fmaf(a, dy, sy);
-            pz = fmaf(a, dz, sz);
-            pixel += 0.5f * sample(px, py, pz);
-            a += step;
-            ++iter;
-        }
-        while (a < am && iter < max_iter) {
-            px = fmaf(a, dx, sx);
-            py = fmaf(a, dy, sy);
-            pz = fmaf(a, dz, sz);
-            pixel += sample(px, py, pz);
-            a += step;
-            ++iter;
-        }
-        pixel *= step;
-        // last segment, :163-179
-        if (pixel > 0.0f) {
-            const float last_val = sample(px, py, pz);
-            pixel -= 0.5f * step * last_val;
-            a -= step;
-            const float last_step = am - a;
-            pixel += 0.5f * last_step * last_val;
-            px = fmaf(am, dx, sx);
-            py = fmaf(am, dy, sy);
-            pz = fmaf(am, dz, sz);
-            pixel += 0.5f * last_step * sample(px, py, pz);
-        }
-        // index length -> mm, :217-219
-        const float spx = spacing_ptr[g * 3 + 2], spy = spacing_ptr[g * 3 + 1], spz = spacing_ptr[g * 3 + 0];
-        pixel *= sqrtf((dx * spx) * (dx * spx) + (dy * spy) * (dy * spy) + (dz * spz) * (dz * spz));
-    }
+    const ConeRay ray = cone_ray_setup(views[(size_t)g * n_proj + p], u, v, X, Y, Z, HW ? -0.5 : 0.0, step,
+                                       spacing_ptr[g * 3 + 2], spacing_ptr[g * 3 + 1], spacing_ptr[g * 3 + 0]);
+    const Sampler<T, HW> sample{vol + (size_t)b * X * Y * Z, tex, X, Y, Z};
+    const float pixel = cone_ray_march<false>(ray, step, sample);
     store_from_float(sino + (((size_t)b * n_proj + p) * H + v) * (size_t)W + u, pixel);
 }
 

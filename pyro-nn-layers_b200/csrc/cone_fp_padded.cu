@@ -16,6 +16,7 @@
 #include <math_constants.h>
 
 #include "common.cuh"
+#include "cone_ray.cuh"
 #include "internal.h"
 
 namespace pyronn {
@@ -96,32 +97,9 @@ __global__ void __launch_bounds__(PB_X *PB_Y)
     if (u >= W || v >= H) return;
     const int g = geom_batch == 1 ? 0 : b;
     const ConeFpView &view = views[(size_t)g * n_proj + p];
-
-    double r[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-        r[k] = view.inv_ar[3 * k + 2] + (double)v * view.inv_ar[3 * k + 1] + (double)u * view.inv_ar[3 * k + 0];
-    const double inv_len = 1.0 / sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) r[k] *= inv_len;
-    const double s[3] = {view.src[0], view.src[1], view.src[2]};
-    const double n_dim[3] = {(double)X, (double)Y, (double)Z};
-    double amin = 0.0, amax = CUDART_INF;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        if (r[k] != 0.0) {
-            const double rc = 1.0 / r[k];
-            const double a0 = (0.0 - s[k]) * rc;
-            const double a1 = (n_dim[k] - s[k]) * rc;
-            if (k == 0) {
-                amin = fmin(a0, a1);
-                amax = fmax(a0, a1);
-            } else {
-                amin = fmax(amin, fmin(a0, a1));
-                amax = fmin(amax, fmax(a0, a1));
-            }
-        }
-    }
+    const float step = step_ptr[g];
+    const ConeRay ray = cone_ray_setup(view, u, v, X, Y, Z, 0.0, step, spacing_ptr[g * 3 + 2], spacing_ptr[g * 3 + 1],
+                                       spacing_ptr[g * 3 + 0]);
     // layout of this view: rays mostly along x -> y-fastest copy
     const double cr0 = view.inv_ar[2] + 0.5 * (W - 1) * view.inv_ar[0] + 0.5 * (H - 1) * view.inv_ar[1];
     const double cr1 = view.inv_ar[5] + 0.5 * (W - 1) * view.inv_ar[3] + 0.5 * (H - 1) * view.inv_ar[4];
@@ -130,50 +108,10 @@ __global__ void __launch_bounds__(PB_X *PB_Y)
     const int sx = along_x ? Yp : 1, sy = along_x ? 1 : Xp, sz = Xp * Yp;
     const T *vol = along_x ? yfast : xfast;
     const float xmax = (float)X + 0.999f, ymax = (float)Y + 0.999f, zmax = (float)Z + 0.999f;
-
-    const float step = step_ptr[g];
-    const float dx = (float)r[0], dy = (float)r[1], dz = (float)r[2];
-    const float ox = (float)s[0], oy = (float)s[1], oz = (float)s[2];
-    float pixel = 0.0f;
-    if (step > 0.0f && step < CUDART_INF_F && amin < amax) {
-        float a = (float)amin;
-        a += step * 0.5f;
-        const float am = (float)amax;
-        const double bound = ((double)am - (double)a) / (double)step + 4.0;
-        const int max_iter = bound > 1.0e8 ? 100000000 : (int)bound;
-        float px = 0.0f, py = 0.0f, pz = 0.0f;
-        int iter = 0;
-        if (a < am) {
-            px = fmaf(a, dx, ox);
-            py = fmaf(a, dy, oy);
-            pz = fmaf(a, dz, oz);
-            pixel += 0.5f * interp3d_padded<T>(vol, px, py, pz, xmax, ymax, zmax, sx, sy, sz);
-            a += step;
-            ++iter;
-        }
-        while (a < am && iter < max_iter) {
-            px = fmaf(a, dx, ox);
-            py = fmaf(a, dy, oy);
-            pz = fmaf(a, dz, oz);
-            pixel += interp3d_padded<T>(vol, px, py, pz, xmax, ymax, zmax, sx, sy, sz);
-            a += step;
-            ++iter;
-        }
-        pixel *= step;
-        if (pixel > 0.0f) {
-            const float last_val = interp3d_padded<T>(vol, px, py, pz, xmax, ymax, zmax, sx, sy, sz);
-            pixel -= 0.5f * step * last_val;
-            a -= step;
-            const float last_step = am - a;
-            pixel += 0.5f * last_step * last_val;
-            px = fmaf(am, dx, ox);
-            py = fmaf(am, dy, oy);
-            pz = fmaf(am, dz, oz);
-            pixel += 0.5f * last_step * interp3d_padded<T>(vol, px, py, pz, xmax, ymax, zmax, sx, sy, sz);
-        }
-        const float spx = spacing_ptr[g * 3 + 2], spy = spacing_ptr[g * 3 + 1], spz = spacing_ptr[g * 3 + 0];
-        pixel *= sqrtf((dx * spx) * (dx * spx) + (dy * spy) * (dy * spy) + (dz * spz) * (dz * spz));
-    }
+    auto sample = [&](float x, float y, float z) {
+        return interp3d_padded<T>(vol, x, y, z, xmax, ymax, zmax, sx, sy, sz);
+    };
+    const float pixel = cone_ray_march<false>(ray, step, sample);
     store_from_float(sino + (((size_t)b * n_proj + p) * H + v) * (size_t)W + u, pixel);
 }
 

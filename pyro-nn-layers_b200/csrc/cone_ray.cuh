@@ -1,0 +1,142 @@
+// cone_ray.cuh -- per-ray set-up and the trapezoid march of the cone-beam
+// forward projector, shared by the projector kernels and by the matched
+// (exact-adjoint) scatter backprojector.
+//
+// Set-up (FP64): direction = normalize(inv_ar (u, v, 1)) in voxel-index space,
+// box entry/exit with the reference's slab tests
+// (cone_projector_3D_CudaKernel.cu.cc:96-132; box [lo, N + lo], lo = 0 for
+// software and -0.5 for hardware interpolation).
+// March (FP32): alpha starts half a step in and advances by `step` in a float
+// (:135-159); the sum is the trapezoid rule with the last segment corrected
+// to the exit point (:160-179).  The reference applies that correction only
+// when the running sum is > 0; `Linear` = true applies it always, which makes
+// the operator linear (it differs only for rays whose sum is <= 0).
+#pragma once
+
+#include <math_constants.h>
+
+#include "internal.h"
+
+namespace pyronn {
+
+struct ConeRay {
+    float dx, dy, dz;  // unit direction (voxel-index space)
+    float ox, oy, oz;  // source (voxel-index space)
+    float a, am;       // first sample parameter (entry + step/2) and exit
+    int max_iter;      // bound on the samples (guards a stagnating float alpha)
+    bool hit;          // the ray has at least one sample
+    float mm_scale;    // |direction (.) spacing|: index length -> mm (:217-219)
+};
+
+__device__ __forceinline__ ConeRay cone_ray_setup(const ConeFpView &view, int u, int v, int X, int Y, int Z,
+                                                  double lo, float step, float spx, float spy, float spz)
+{
+    double r[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        r[k] = view.inv_ar[3 * k + 2] + (double)v * view.inv_ar[3 * k + 1] + (double)u * view.inv_ar[3 * k + 0];
+    const double inv_len = 1.0 / sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) r[k] *= inv_len;
+    const double n_dim[3] = {(double)X, (double)Y, (double)Z};
+    double amin = 0.0, amax = CUDART_INF;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (r[k] != 0.0) {
+            const double rc = 1.0 / r[k];
+            const double a0 = (lo - view.src[k]) * rc;
+            const double a1 = (n_dim[k] + lo - view.src[k]) * rc;
+            if (k == 0) {
+                amin = fmin(a0, a1);
+                amax = fmax(a0, a1);
+            } else {
+                amin = fmax(amin, fmin(a0, a1));
+                amax = fmin(amax, fmax(a0, a1));
+            }
+        }
+    }
+    ConeRay ray;
+    ray.dx = (float)r[0];
+    ray.dy = (float)r[1];
+    ray.dz = (float)r[2];
+    ray.ox = (float)view.src[0];
+    ray.oy = (float)view.src[1];
+    ray.oz = (float)view.src[2];
+    float a = (float)amin;
+    a += step * 0.5f;
+    ray.a = a;
+    ray.am = (float)amax;
+    ray.hit = step > 0.0f && step < CUDART_INF_F && amin < amax && a < ray.am;
+    const double bound = ray.hit ? ((double)ray.am - (double)a) / (double)step + 4.0 : 0.0;
+    ray.max_iter = bound > 1.0e8 ? 100000000 : (int)bound;
+    ray.mm_scale = sqrtf((ray.dx * spx) * (ray.dx * spx) + (ray.dy * spy) * (ray.dy * spy) +
+                         (ray.dz * spz) * (ray.dz * spz));
+    return ray;
+}
+
+// sum of one ray; sample(x, y, z) returns the interpolated value at a point
+template <bool Linear, typename F>
+__device__ __forceinline__ float cone_ray_march(const ConeRay &ray, float step, const F &sample)
+{
+    if (!ray.hit) return 0.0f;
+    float a = ray.a;
+    float px = fmaf(a, ray.dx, ray.ox), py = fmaf(a, ray.dy, ray.oy), pz = fmaf(a, ray.dz, ray.oz);
+    float pixel = 0.5f * sample(px, py, pz);
+    a += step;
+    int iter = 1;
+    while (a < ray.am && iter < ray.max_iter) {
+        px = fmaf(a, ray.dx, ray.ox);
+        py = fmaf(a, ray.dy, ray.oy);
+        pz = fmaf(a, ray.dz, ray.oz);
+        pixel += sample(px, py, pz);
+        a += step;
+        ++iter;
+    }
+    pixel *= step;
+    if (Linear || pixel > 0.0f) {
+        const float last_val = sample(px, py, pz);
+        pixel -= 0.5f * step * last_val;
+        a -= step;
+        const float last_step = ray.am - a;
+        pixel += 0.5f * last_step * last_val;
+        px = fmaf(ray.am, ray.dx, ray.ox);
+        py = fmaf(ray.am, ray.dy, ray.oy);
+        pz = fmaf(ray.am, ray.dz, ray.oz);
+        pixel += 0.5f * last_step * sample(px, py, pz);
+    }
+    return pixel * ray.mm_scale;
+}
+
+// Visits every sample point of the linear march with the weight the sample
+// carries in the (scaled) line integral: visit(x, y, z, weight).  The sum of
+// weight * value over the visits equals cone_ray_march<true>.
+template <typename F>
+__device__ __forceinline__ void cone_ray_weights(const ConeRay &ray, float step, const F &visit)
+{
+    if (!ray.hit) return;
+    float a = ray.a;
+    const float s = ray.mm_scale;
+    // the final sample's weight is only known at the end: hold it back
+    float px = fmaf(a, ray.dx, ray.ox), py = fmaf(a, ray.dy, ray.oy), pz = fmaf(a, ray.dz, ray.oz);
+    float w_held = 0.5f * step;
+    a += step;
+    int iter = 1;
+    while (a < ray.am && iter < ray.max_iter) {
+        visit(px, py, pz, w_held * s);
+        px = fmaf(a, ray.dx, ray.ox);
+        py = fmaf(a, ray.dy, ray.oy);
+        pz = fmaf(a, ray.dz, ray.oz);
+        w_held = step;
+        a += step;
+        ++iter;
+    }
+    a -= step;
+    const float last_step = ray.am - a;
+    // last sample: its march weight, minus the half step the correction
+    // removes, plus half the last segment
+    visit(px, py, pz, (w_held - 0.5f * step + 0.5f * last_step) * s);
+    visit(fmaf(ray.am, ray.dx, ray.ox), fmaf(ray.am, ray.dy, ray.oy), fmaf(ray.am, ray.dz, ray.oz),
+          0.5f * last_step * s);
+}
+
+}  // namespace pyronn

@@ -63,6 +63,11 @@ cudaError_t launch_cone_fp_padded(const void *volume, void *sinogram, int in_dty
                                   const ConeFpView *views, const float *step, const float *spacing, void *scratch,
                                   cudaStream_t stream);
 
+// matched (exact-adjoint) scatter backprojector (cone_matched.cu); FP32 output
+cudaError_t launch_cone_scatter(const void *sinogram, float *volume, int in_dtype, const Dims3D &d,
+                                const ConeFpView *views, const float *step, const float *spacing,
+                                cudaStream_t stream);
+
 // TMA-staged software backprojector (cone_bp_tma.cu); err = device error flag
 bool cone_bp_tma_supported(const void *sinogram, int in_dtype, const Dims3D &d);
 cudaError_t launch_cone_bp_tma(const void *sinogram, void *volume, int in_dtype, int out_dtype, const Dims3D &d,

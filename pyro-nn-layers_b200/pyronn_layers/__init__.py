@@ -12,6 +12,7 @@ They run hand-written sm_100a CUDA kernels through the C ABI of
 """
 from .ops import (  # noqa: F401
     cone_backprojection3d,
+    cone_backprojection3d_matched,
     cone_projection3d,
     fan_backprojection2d,
     fan_projection2d,
@@ -29,6 +30,7 @@ __all__ = [
     "fan_backprojection2d",
     "cone_projection3d",
     "cone_backprojection3d",
+    "cone_backprojection3d_matched",
     "release_cached_arrays",
     "PyronnError",
     "geometry",

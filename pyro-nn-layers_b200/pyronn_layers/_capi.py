@@ -45,6 +45,9 @@ PROTOTYPES = {
     "pyronn_cone_backprojection3d_workspace_size": (_SZ, [_I] * 10),
     "pyronn_cone_backprojection3d": (
         _I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _P, _SZ, _P]),
+    "pyronn_cone_backprojection3d_matched_workspace_size": (_SZ, [_I, _I]),
+    "pyronn_cone_backprojection3d_matched": (
+        _I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _I, _P, _SZ, _P]),
 }
 
 

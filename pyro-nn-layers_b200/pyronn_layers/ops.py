@@ -218,6 +218,23 @@ def _run_cone(forward: bool, x: torch.Tensor, out_dims, geo: GeometryCone, hardw
     return out
 
 
+def _run_matched(p: torch.Tensor, vol_dims, geo: GeometryCone) -> torch.Tensor:
+    batch = p.shape[0]
+    dev = p.device
+    n_proj, det_h, det_w = p.shape[1:]
+    vol_z, vol_y, vol_x = vol_dims
+    out = torch.empty((batch, vol_z, vol_y, vol_x), dtype=torch.float32, device=dev)
+    fn = "pyronn_cone_backprojection3d_matched"
+    ws_bytes = _capi.workspace_size(fn, geo.g, n_proj)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    with torch.cuda.device(dev):
+        _capi.call(fn, p.data_ptr(), out.data_ptr(), storage_code(p.dtype), batch, n_proj, det_h, det_w, vol_z, vol_y,
+                   vol_x, geo.volume_origin.data_ptr(), geo.volume_spacing.data_ptr(),
+                   geo.projection_matrices.data_ptr(), geo.step_size.data_ptr(), geo.g, ws.data_ptr(), ws_bytes,
+                   _stream(dev))
+    return out
+
+
 # ------------------------------------------------------------- autograd
 
 
@@ -239,19 +256,25 @@ class _Op2D(torch.autograd.Function):
 
 class _OpCone(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, x, forward_op, out_dims, geo, hardware_interp, out_dtype):
+    def forward(ctx, x, forward_op, out_dims, geo, hardware_interp, out_dtype, matched=False):
         ctx.forward_op = forward_op
         ctx.in_dims = tuple(x.shape[1:])
         ctx.in_dtype = x.dtype
         ctx.geo = geo
         ctx.hardware_interp = hardware_interp
+        ctx.matched = matched
+        if matched and not forward_op:
+            return _run_matched(x, out_dims, geo).to(out_dtype or torch.float32)
         return _run_cone(forward_op, x, out_dims, geo, hardware_interp, out_dtype)
 
     @staticmethod
     def backward(ctx, grad):
         g = grad.contiguous()
-        gx = _run_cone(not ctx.forward_op, g, ctx.in_dims, ctx.geo, ctx.hardware_interp, ctx.in_dtype)
-        return gx, None, None, None, None, None
+        if ctx.matched and ctx.forward_op:
+            gx = _run_matched(g, ctx.in_dims, ctx.geo).to(ctx.in_dtype)
+        else:
+            gx = _run_cone(not ctx.forward_op, g, ctx.in_dims, ctx.geo, ctx.hardware_interp, ctx.in_dtype)
+        return gx, None, None, None, None, None, None
 
 
 # ----------------------------------------------------------- public op surface
@@ -304,17 +327,38 @@ def fan_backprojection2d(sinogram, volume_shape, volume_origin, detector_origin,
 
 
 def cone_projection3d(volume, projection_shape, volume_origin, volume_spacing, projection_matrices, step_size,
-                      projection_multiplier, hardware_interp=False, name=None, out_dtype=None):
+                      projection_multiplier, hardware_interp=False, name=None, out_dtype=None, matched_adjoint=False):
     """A x for 3D cone beam: [B, Z, Y, X] -> [B, n_proj, det_h, det_w].
 
     projection_shape = (n_proj, det_h, det_w) (cc/ops/cone_projector_3D_OPKernel.cc:219-226);
     step_size in voxels along the ray; projection_multiplier is unused by the
-    forward op, as in the reference."""
+    forward op, as in the reference.  matched_adjoint=True makes the gradient
+    the exact transpose (cone_backprojection3d_matched) instead of the paired
+    voxel-driven backprojector (software interpolation only)."""
     x = _check_data(volume, 4, "volume")
     n_proj, det_h, det_w = _shape(projection_shape, 3, "projection_shape")
+    if matched_adjoint and hardware_interp:
+        raise ValueError("matched_adjoint is the transpose of the software-interpolation projector")
     geo = GeometryCone(x.shape[0], x.device, volume_origin, volume_spacing, projection_matrices, step_size,
                        projection_multiplier, n_proj)
-    return _OpCone.apply(x, True, (n_proj, det_h, det_w), geo, bool(hardware_interp), out_dtype)
+    return _OpCone.apply(x, True, (n_proj, det_h, det_w), geo, bool(hardware_interp), out_dtype,
+                         bool(matched_adjoint))
+
+
+def cone_backprojection3d_matched(sinogram, volume_shape, volume_origin, volume_spacing, projection_matrices,
+                                  step_size, projection_multiplier=None, name=None, out_dtype=None):
+    """Exact transpose of the software-interpolation cone_projection3d:
+    [B, n_proj, det_h, det_w] -> [B, Z, Y, X] (FP32 accumulation by atomics).
+
+    No counterpart in the reference (its voxel-driven backprojector is not the
+    transpose of its projector).  projection_multiplier is accepted for
+    signature symmetry and not applied."""
+    p = _check_data(sinogram, 4, "sinogram")
+    vol_z, vol_y, vol_x = _shape(volume_shape, 3, "volume_shape")
+    mult = 1.0 if projection_multiplier is None else projection_multiplier
+    geo = GeometryCone(p.shape[0], p.device, volume_origin, volume_spacing, projection_matrices, step_size, mult,
+                       p.shape[1])
+    return _OpCone.apply(p, False, (vol_z, vol_y, vol_x), geo, False, out_dtype, True)
 
 
 def cone_backprojection3d(sinogram, volume_shape, volume_origin, volume_spacing, projection_matrices, step_size,

@@ -125,3 +125,19 @@ def test_oracle_matches_reference_cone(name, hw):
     assert rel_l2(sino, g["sinogram_ref_hw%d" % hw]) < tol
     vol = oracle.cone_backprojection3d(g["sinogram_in"], g["volume"].shape[1:], *args, hardware_interp=hw)
     assert rel_l2(vol, g["volume_ref_hw%d" % hw]) < tol
+
+
+def test_matched_backprojection_is_the_transpose():
+    """<A x, y> = <x, A^T y> for the forward projector and the matched
+    backprojector (positive x: the reference's end correction always runs)."""
+    geo = geometry.ConeBeam3D((10, 12, 14), (1.0, 0.9, 1.1), (16, 18), (1.3, 1.3), 6, 120.0, 200.0, step_size=0.7)
+    rng = np.random.Generator(np.random.PCG64(4))
+    x = rng.uniform(0.1, 1, (1,) + geo.volume_shape).astype(np.float32)
+    y = rng.uniform(-1, 1, (1,) + geo.detector_shape).astype(np.float32)
+    ax = oracle.cone_projection3d(x, geo.detector_shape, *geo.args())
+    aty = oracle.cone_backprojection3d_matched(y, geo.volume_shape, *geo.args())
+    lhs, rhs = float((ax * y).sum()), float((x.astype(np.float64) * aty).sum())
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+    # the reference's voxel-driven backprojector is not the transpose
+    bp = oracle.cone_backprojection3d(y, geo.volume_shape, *geo.args())
+    assert abs(float((x.astype(np.float64) * bp).sum()) - lhs) > 1e-3 * abs(lhs)
