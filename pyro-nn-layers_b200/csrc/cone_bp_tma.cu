@@ -164,7 +164,10 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
                        int W, int H, int n_proj, int geom_batch, unsigned *__restrict__ err)
 {
     extern __shared__ __align__(128) unsigned char dyn_smem[];
-    T(*tiles)[BP_K][BOX_ELEMS] = reinterpret_cast<T(*)[BP_K][BOX_ELEMS]>(dyn_smem);  // [2][BP_K][BOX_ELEMS]
+    // TMA destinations must be 128-byte aligned: round the base up (the
+    // launch reserves 128 spare bytes); every tile is a multiple of 128 bytes
+    unsigned char *tile_base = dyn_smem + ((128u - (smem_addr(dyn_smem) & 127u)) & 127u);
+    T(*tiles)[BP_K][BOX_ELEMS] = reinterpret_cast<T(*)[BP_K][BOX_ELEMS]>(tile_base);  // [2][BP_K][BOX_ELEMS]
     __shared__ __align__(16) ViewMeta meta[2][BP_K];
     __shared__ __align__(8) uint64_t full[2];
 
@@ -331,7 +334,8 @@ cudaError_t launch_typed(const void *sinogram, void *volume, const Dims3D &d, co
     const int zblocks = (d.vol_z + TB_Z - 1) / TB_Z;
     const dim3 block(TB_X, TB_Y, 1);
     const dim3 grid((d.vol_x + TB_X - 1) / TB_X, (d.vol_y + TB_Y - 1) / TB_Y, zblocks * d.batch);
-    const size_t smem = 2 * BP_K * BOX_ELEMS * sizeof(Tin);
+    static_assert((BOX_ELEMS * sizeof(float)) % 128 == 0 && (BOX_ELEMS * 2) % 128 == 0, "tile alignment");
+    const size_t smem = 2 * BP_K * BOX_ELEMS * sizeof(Tin) + 128;
     static bool attr_set = false;  // per instantiation
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(cone_bp_tma_kernel<Tin, Tout>,

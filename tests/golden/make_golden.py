@@ -35,11 +35,24 @@ from pyronn_layers import geometry, phantoms  # noqa: E402
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
+# every device buffer handed to the reference stays referenced here until the
+# script ends: a temporary freed before the call would hand its block to the
+# next allocation and the reference would read the wrong data
+_KEEP = []
+
+
 def dev(a, slack=0):
     a = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
     t = torch.zeros(a.size + slack, dtype=torch.float32, device="cuda")
     t[: a.size] = torch.from_numpy(a.reshape(-1)).cuda()
+    _KEEP.append(t)
     return t
+
+
+def check_geometry(step_like):
+    """The reference's march loops forever on a zero step: refuse one."""
+    if not np.all(np.asarray(step_like, np.float64) > 0):
+        raise ValueError("non-positive spacing/step would stall the reference kernel")
 
 
 def ptr(t):
@@ -62,6 +75,7 @@ def case_parallel(L):
     B, Y, X, n_proj, W = 2, 64, 64, 60, 95
     vols = np.stack([phantoms.ellipse_phantom_2d((Y, X), (1.0, 1.0), seed=10 + b, n=6)[0] for b in range(B)])
     vs = np.array([[1.0, 1.0], [1.0, 1.0]], np.float32)
+    check_geometry(vs)
     vo = np.stack([geometry.centered_origin((Y, X), vs[b]) for b in range(B)])
     ds = np.array([[1.0], [1.0]], np.float32)
     do = np.stack([geometry.detector_origin_1d(W, 1.0)] * B)
@@ -83,6 +97,7 @@ def case_parallel(L):
 def case_fan(L):
     B, Y, X, n_proj, W = 2, 64, 64, 72, 128
     vs = np.array([[0.5, 0.5], [0.5, 0.5]], np.float32)
+    check_geometry(vs)
     vols = np.stack([phantoms.ellipse_phantom_2d((Y, X), (0.5, 0.5), seed=20 + b, n=6)[0] for b in range(B)])
     vo = np.stack([geometry.centered_origin((Y, X), vs[b]) for b in range(B)])
     ds = np.array([[0.5], [0.5]], np.float32)
@@ -116,6 +131,8 @@ def cone_case(L, name, vol_shape, spacing, det_shape, det_spacing, n_proj, sid, 
     vo, vs, P, st, mu = (np.asarray(a, np.float32) for a in g.args())
     vo, vs, st, mu = vo[None], vs[None], st[None], mu[None]
     P = P[None]
+    check_geometry(vs)
+    check_geometry(st)
     out = {}
     for hw in (0, 1):
         sino = torch.zeros(n_proj * H * W, device="cuda")
