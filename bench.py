@@ -460,13 +460,52 @@ def run_ours(args, cfg):
         dist.destroy_process_group()
 
 
+def run_serving(args):
+    """Serving stream (config 5): a seeded Poisson trace of mixed jobs through
+    the continuous-batching server and through the plain one-job-per-launch
+    FP32 path on the same GPU; reports p50/p99 latency and aggregate GUPS."""
+    import torch
+
+    from pyronn_layers import serving
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    geos = serving.standard_geometries()
+    trace = serving.poisson_trace(args.requests, args.rate, seed=7)
+    jobs = serving.make_jobs(trace, geos, seed=1)
+    # warm-up: one of each class through the server (graphs, caches, lazy set-up)
+    warm = serving.make_jobs([(0.0, c) for c in sorted({c for _, c in trace}, key=str)], geos, seed=1)
+    server = serving.ProjectorServer(geos, device=dev, keep_results=False)
+    server.run_trace(warm, realtime=False)
+    server.batches, server.batch_sizes = 0, []
+    with ClockSampler(physical_gpu_index(dev.index or 0)) as clk:
+        s_srv = server.run_trace(jobs, realtime=True)
+    jobs_plain = serving.make_jobs(trace, geos, seed=1)
+    s_plain = serving.run_plain(jobs_plain, geos, device=dev, realtime=True)
+    line = {
+        "metric": METRIC, "value": s_srv.gups, "unit": "GUPS", "n_gpus": 1, "steps": args.requests, "warmup": 1,
+        "ms_per_step": s_srv.wall_s * 1e3 / max(1, args.requests), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "storage": "fp32/bf16 mix", "data": "synthetic",
+        "config": {"workload": "serving", "requests": args.requests, "rate_hz": args.rate,
+                   "mix": "60% fan 512^2 (360 views, 1024 px), 30% cone 128^3 (180 views, 256^2), 10% cone 256^3 "
+                          "(360 views, 512^2); forward/back 50/50; FP32/BF16 50/50",
+                   "arrivals": "Poisson, seed 7"},
+        "serving": s_srv.as_dict(),
+        "plain_one_job_per_launch_fp32": s_plain.as_dict(),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cone512")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving"], default="cone512")
+    ap.add_argument("--requests", type=int, default=2000, help="serving: number of requests")
+    ap.add_argument("--rate", type=float, default=100.0, help="serving: Poisson arrival rate (1/s)")
     ap.add_argument("--storage", choices=["bf16", "fp16", "fp32"], default="bf16")
     ap.add_argument("--hardware-interp", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -474,6 +513,12 @@ def main(argv=None):
                     help="dram bytes per launch of the dominant kernel from an ncu capture")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)  # at least 3 untimed warm-up steps
+    if args.workload == "serving":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the serving stream has no CPU reference arm"}))
+            return
+        run_serving(args)
+        return
     cfg = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, cfg)

@@ -87,6 +87,27 @@ cudaError_t dispatch_dtypes(int in_dtype, int out_dtype, F &&f)
     }
 }
 
+// floor and fraction without the conversion pipe: for |x| < 2^22,
+// y = (x - 0.5) + 1.5 * 2^23 rounds to the integer nearest x - 0.5, i.e.
+// floor(x) -- at an exact integer x = k the tie may give k - 1 with
+// frac = 1, which interpolates to exactly the same value (lerp(a, b, 1) == b
+// and lerp(a, b, 0) == a in the FMA form).  The integer is read from y's
+// mantissa.  Four FADDs and an integer add instead of FRND + F2I.
+struct FloorFrac {
+    int i;
+    float f;  // x - i, exact
+};
+
+__device__ __forceinline__ FloorFrac floor_frac(float x)
+{
+    const float magic = 12582912.0f;  // 1.5 * 2^23
+    const float y = __fadd_rn(__fadd_rn(x, -0.5f), magic);
+    FloorFrac r;
+    r.i = __float_as_int(y) - 0x4B400000;
+    r.f = __fadd_rn(x, -__fadd_rn(y, -magic));
+    return r;
+}
+
 // Approximate reciprocal (one MUFU op, <= 1 ulp).
 __device__ __forceinline__ float fast_rcp(float x)
 {

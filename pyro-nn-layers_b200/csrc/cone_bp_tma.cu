@@ -32,7 +32,7 @@ constexpr int TB_X = 32;
 constexpr int TB_Y = 8;
 constexpr int TB_Z = 8;  // voxels per thread along z
 constexpr int BP_K = 4;  // views per pass
-constexpr int BOX_W = 64;
+constexpr int BOX_W = 72;  // 72-element rows shift banks between rows (64 would alias them)
 constexpr int BOX_H = 24;
 constexpr int BOX_ELEMS = BOX_W * BOX_H;
 
@@ -246,9 +246,9 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
                     // local box coordinates; the subtraction of an integer is exact
                     const float lu = fmaf(r0.z, fz, ub) * rw - u0;
                     const float lv = fmaf(r1.z, fz, vb) * rw - v0;
-                    const float fu = floorf(lu), fv = floorf(lv);
-                    const float tx = lu - fu, ty = lv - fv;
-                    unsigned idx = (unsigned)(__float2int_rz(fv) * BOX_W + __float2int_rz(fu));
+                    const FloorFrac fu = floor_frac(lu), fv = floor_frac(lv);
+                    const float tx = fu.f, ty = fv.f;
+                    unsigned idx = (unsigned)(fv.i * BOX_W + fu.i);
                     idx = min(idx, MAX_IDX);  // memory safety only: the margin keeps idx in range
                     const float p00 = smem_to_float(tile + idx);
                     const float p01 = smem_to_float(tile + idx + 1);

@@ -56,32 +56,110 @@ __global__ void __launch_bounds__(PAD_TILE *8) pad_volume_kernel(const T *__rest
     }
 }
 
-template <typename T>
-__device__ __forceinline__ float interp3d_padded(const T *__restrict__ vol, float x, float y, float z, float xmax,
-                                                 float ymax, float zmax, int sx, int sy, int sz)
+// Trilinear interpolation from a padded copy.  FASTY selects the y-fastest
+// layout; the tap along the fastest axis is then the next element (an
+// immediate offset), the others are a row / a slice away.  `origin` points at
+// padded (1, 1, 1), i.e. source voxel (0, 0, 0); any sample whose floor lies
+// in [-1, N] keeps all its taps inside the padded copy.
+template <typename T, bool FASTY>
+struct PaddedSampler {
+    const T *origin;
+    int s_row, s_slice;  // element strides of the slow in-slice axis and of z
+
+    __device__ __forceinline__ float operator()(float x, float y, float z) const
+    {
+        const FloorFrac fx = floor_frac(x), fy = floor_frac(y), fz = floor_frac(z);
+        const int fast = FASTY ? fy.i : fx.i, slow = FASTY ? fx.i : fy.i;
+        const T *p = origin + (fz.i * s_slice + slow * s_row + fast);
+        const T *q = p + s_slice;
+        const float p000 = load_as_float(p), p_f = load_as_float(p + 1);
+        const float p0s = load_as_float(p + s_row), p_fs = load_as_float(p + s_row + 1);
+        const float p100 = load_as_float(q), q_f = load_as_float(q + 1);
+        const float q0s = load_as_float(q + s_row), q_fs = load_as_float(q + s_row + 1);
+        // the reference's order: lerp in z, then y, then x
+        const float c00 = lerp_ref(p000, p100, fz.f), c_f = lerp_ref(p_f, q_f, fz.f);
+        const float c_s = lerp_ref(p0s, q0s, fz.f), c_fs = lerp_ref(p_fs, q_fs, fz.f);
+        if (FASTY) {  // fast = y, slow = x
+            const float x0 = lerp_ref(c00, c_f, fy.f), x1 = lerp_ref(c_s, c_fs, fy.f);
+            return lerp_ref(x0, x1, fx.f);
+        } else {      // fast = x, slow = y
+            const float y0 = lerp_ref(c00, c_s, fy.f), y1 = lerp_ref(c_f, c_fs, fy.f);
+            return lerp_ref(y0, y1, fx.f);
+        }
+    }
+};
+
+// Generic clamped sample for rays whose end points are not proven inside the
+// padded range: clamping to [-1, N + 0.999] changes no value (outside
+// [-1, N + 1) all taps are border zeros) and keeps every tap in the copy.
+template <typename T, bool FASTY>
+struct ClampedSampler {
+    PaddedSampler<T, FASTY> s;
+    float xmax, ymax, zmax;
+    __device__ __forceinline__ float operator()(float x, float y, float z) const
+    {
+        return s(fminf(fmaxf(x, -1.0f), xmax), fminf(fmaxf(y, -1.0f), ymax), fminf(fmaxf(z, -1.0f), zmax));
+    }
+};
+
+// The reference's march (cone_ray.cuh) with the main loop taking two
+// samples per iteration, so the gathers of both are in flight together; the
+// alpha sequence and the order of the additions are unchanged.
+template <typename F>
+__device__ __forceinline__ float march_x2(const ConeRay &ray, float step, const F &sample)
 {
-    // clamping to [-1, N + 0.999] keeps every tap inside the padded copy and
-    // changes no value: outside [-1, N + 1) all taps are border zeros anyway
-    x = fminf(fmaxf(x, -1.0f), xmax);
-    y = fminf(fmaxf(y, -1.0f), ymax);
-    z = fminf(fmaxf(z, -1.0f), zmax);
-    const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
-    const float tx = x - fx, ty = y - fy, tz = z - fz;
-    const int base = ((int)fx + 1) * sx + ((int)fy + 1) * sy + ((int)fz + 1) * sz;
-    const T *p = vol + base;
-    const float p000 = load_as_float(p);
-    const float p001 = load_as_float(p + sx);
-    const float p010 = load_as_float(p + sy);
-    const float p011 = load_as_float(p + sy + sx);
-    const float p100 = load_as_float(p + sz);
-    const float p101 = load_as_float(p + sz + sx);
-    const float p110 = load_as_float(p + sz + sy);
-    const float p111 = load_as_float(p + sz + sy + sx);
-    const float p00 = lerp_ref(p000, p100, tz);
-    const float p01 = lerp_ref(p001, p101, tz);
-    const float p10 = lerp_ref(p010, p110, tz);
-    const float p11 = lerp_ref(p011, p111, tz);
-    return lerp_ref(lerp_ref(p00, p10, ty), lerp_ref(p01, p11, ty), tx);
+    if (!ray.hit) return 0.0f;
+    float a = ray.a;
+    float px = fmaf(a, ray.dx, ray.ox), py = fmaf(a, ray.dy, ray.oy), pz = fmaf(a, ray.dz, ray.oz);
+    float pixel = 0.5f * sample(px, py, pz);
+    a += step;
+    int iter = 1;
+    while (a < ray.am && iter < ray.max_iter) {
+        const float a1 = a + step;
+        if (a1 < ray.am && iter + 1 < ray.max_iter) {
+            const float qx = fmaf(a, ray.dx, ray.ox), qy = fmaf(a, ray.dy, ray.oy), qz = fmaf(a, ray.dz, ray.oz);
+            px = fmaf(a1, ray.dx, ray.ox);
+            py = fmaf(a1, ray.dy, ray.oy);
+            pz = fmaf(a1, ray.dz, ray.oz);
+            const float v0 = sample(qx, qy, qz), v1 = sample(px, py, pz);
+            pixel += v0;
+            pixel += v1;
+            a = a1 + step;
+            iter += 2;
+        } else {
+            px = fmaf(a, ray.dx, ray.ox);
+            py = fmaf(a, ray.dy, ray.oy);
+            pz = fmaf(a, ray.dz, ray.oz);
+            pixel += sample(px, py, pz);
+            a += step;
+            ++iter;
+        }
+    }
+    pixel *= step;
+    if (pixel > 0.0f) {
+        const float last_val = sample(px, py, pz);
+        pixel -= 0.5f * step * last_val;
+        a -= step;
+        const float last_step = ray.am - a;
+        pixel += 0.5f * last_step * last_val;
+        px = fmaf(ray.am, ray.dx, ray.ox);
+        py = fmaf(ray.am, ray.dy, ray.oy);
+        pz = fmaf(ray.am, ray.dz, ray.oz);
+        pixel += 0.5f * last_step * sample(px, py, pz);
+    }
+    return pixel * ray.mm_scale;
+}
+
+// true when every point of the FP32 march lies in [-0.5, N + 0.5]: its end
+// points do (the segment between is convex) -- checked once per ray
+__device__ __forceinline__ bool march_inside(const ConeRay &r, int X, int Y, int Z)
+{
+    if (!r.hit) return true;
+    const float x0 = fmaf(r.a, r.dx, r.ox), y0 = fmaf(r.a, r.dy, r.oy), z0 = fmaf(r.a, r.dz, r.oz);
+    const float x1 = fmaf(r.am, r.dx, r.ox), y1 = fmaf(r.am, r.dy, r.oy), z1 = fmaf(r.am, r.dz, r.oz);
+    const float lo = -0.5f;
+    return fminf(x0, x1) >= lo && fminf(y0, y1) >= lo && fminf(z0, z1) >= lo && fmaxf(x0, x1) <= X + 0.5f &&
+           fmaxf(y0, y1) <= Y + 0.5f && fmaxf(z0, z1) <= Z + 0.5f;
 }
 
 template <typename T, typename Tout>
@@ -100,18 +178,22 @@ __global__ void __launch_bounds__(PB_X *PB_Y)
     const float step = step_ptr[g];
     const ConeRay ray = cone_ray_setup(view, u, v, X, Y, Z, 0.0, step, spacing_ptr[g * 3 + 2], spacing_ptr[g * 3 + 1],
                                        spacing_ptr[g * 3 + 0]);
-    // layout of this view: rays mostly along x -> y-fastest copy
+    // layout of this view (uniform per block): rays mostly along x -> y-fastest copy
     const double cr0 = view.inv_ar[2] + 0.5 * (W - 1) * view.inv_ar[0] + 0.5 * (H - 1) * view.inv_ar[1];
     const double cr1 = view.inv_ar[5] + 0.5 * (W - 1) * view.inv_ar[3] + 0.5 * (H - 1) * view.inv_ar[4];
     const bool along_x = fabs(cr0) > fabs(cr1);
     const int Xp = X + 3, Yp = Y + 3;
-    const int sx = along_x ? Yp : 1, sy = along_x ? 1 : Xp, sz = Xp * Yp;
-    const T *vol = along_x ? yfast : xfast;
+    const int s_slice = Xp * Yp;
+    const bool inside = march_inside(ray, X, Y, Z);
     const float xmax = (float)X + 0.999f, ymax = (float)Y + 0.999f, zmax = (float)Z + 0.999f;
-    auto sample = [&](float x, float y, float z) {
-        return interp3d_padded<T>(vol, x, y, z, xmax, ymax, zmax, sx, sy, sz);
-    };
-    const float pixel = cone_ray_march<false>(ray, step, sample);
+    float pixel;
+    if (along_x) {
+        const PaddedSampler<T, true> s{yfast + s_slice + Yp + 1, Yp, s_slice};
+        pixel = inside ? march_x2(ray, step, s) : march_x2(ray, step, ClampedSampler<T, true>{s, xmax, ymax, zmax});
+    } else {
+        const PaddedSampler<T, false> s{xfast + s_slice + Xp + 1, Xp, s_slice};
+        pixel = inside ? march_x2(ray, step, s) : march_x2(ray, step, ClampedSampler<T, false>{s, xmax, ymax, zmax});
+    }
     store_from_float(sino + (((size_t)b * n_proj + p) * H + v) * (size_t)W + u, pixel);
 }
 
