@@ -200,6 +200,39 @@ PYRONN_API int pyronn_cone_backprojection3d_matched(const void *sinogram, float 
                                                     const float *step_size, int geom_batch, void *workspace,
                                                     size_t workspace_bytes, void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Cone backprojection that allocates nothing.  No counterpart in the
+ * reference (whose launchers cudaMalloc per call, the out-of-memory trap its
+ * README warns about when TensorFlow's allocator owns the GPU).
+ *
+ * For callers that cannot provide a workspace or call cudaMalloc: a host
+ * framework whose allocator owns the device memory and cannot lend a buffer
+ * to foreign code, or a real-time loop that must not allocate (cudaMalloc
+ * synchronises the device).  Same arguments and result as
+ * pyronn_cone_backprojection3d with hardware_interp = 0, minus the workspace:
+ * the scratch (prepared projection matrices and the error flag) lives in a
+ * fixed array of device global memory inside the library, which every GPU
+ * that loads the library holds until process exit.
+ *   - geom_batch * n_proj must not exceed PYRONN_NOALLOC_MAX_VIEWS (8192
+ *     views, 384 KiB of scratch); larger requests return
+ *     PYRONN_ERROR_UNSUPPORTED;
+ *   - software interpolation only (texture arrays would be allocations);
+ *   - the first call on a device looks up the array's device address, so make
+ *     that call before capturing a stream;
+ *   - all calls on a device share the array (it keeps the last call's
+ *     contents; each call rewrites what it reads): calls that overlap on the
+ *     same GPU race and must be serialised by the caller.
+ * ------------------------------------------------------------------------- */
+#define PYRONN_NOALLOC_MAX_VIEWS 8192
+
+PYRONN_API int pyronn_cone_backprojection3d_noalloc(const void *sinogram, void *volume, int in_dtype,
+                                                    int out_dtype, int batch, int n_proj, int det_h, int det_w,
+                                                    int vol_z, int vol_y, int vol_x, const float *volume_origin,
+                                                    const float *volume_spacing,
+                                                    const float *projection_matrices, const float *step_size,
+                                                    const float *projection_multiplier, int geom_batch,
+                                                    void *stream);
+
 #ifdef __cplusplus
 }
 #endif

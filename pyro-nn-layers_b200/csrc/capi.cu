@@ -28,10 +28,32 @@ size_t dtype_size(int dtype)
 using namespace pyronn;
 
 namespace {
+int fail(int status, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
+int cuda_fail(cudaError_t e, const char *what);
+}  // namespace
+
+namespace pyronn {
+
+int report_error(int status, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    return fail(status, "%s", buf);
+}
+
+int report_cuda_error(cudaError_t e, const char *what)
+{
+    return cuda_fail(e, what);
+}
+
+}  // namespace pyronn
+
+namespace {
 
 thread_local std::string t_last_error;
-
-int fail(int status, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
 
 int fail(int status, const char *fmt, ...)
 {

@@ -88,4 +88,8 @@ int array_cache_clear();
 
 size_t dtype_size(int dtype);
 
+// record a failure as the calling thread's last error (capi.cu); return status
+int report_error(int status, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
+int report_cuda_error(cudaError_t e, const char *what);
+
 }  // namespace pyronn

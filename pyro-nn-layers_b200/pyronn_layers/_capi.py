@@ -48,7 +48,11 @@ PROTOTYPES = {
     "pyronn_cone_backprojection3d_matched_workspace_size": (_SZ, [_I, _I]),
     "pyronn_cone_backprojection3d_matched": (
         _I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _I, _P, _SZ, _P]),
+    "pyronn_cone_backprojection3d_noalloc": (
+        _I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _P]),
 }
+
+NOALLOC_MAX_VIEWS = 8192  # PYRONN_NOALLOC_MAX_VIEWS
 
 
 class PyronnError(RuntimeError):
