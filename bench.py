@@ -497,13 +497,89 @@ def run_serving(args):
     print(json.dumps(line))
 
 
+FAN2D = dict(batch=64, volume=(512, 512), pixel_mm=0.5, views=360, detector=1024, det_mm=0.5, sid_mm=750.0,
+             sdd_mm=1200.0)
+
+
+def run_fan2d(args):
+    """2D fan-beam batch (config 2): 64 independent 512^2 slices at 0.5 mm,
+    360 views over 2 pi, flat 1024-px detector at 0.5 mm, SID 750 / SDD 1200;
+    one step = FanProjection2D of the batch + FanBackprojection2D of its
+    sinograms.  GUPS = 2 * 64 * 512^2 * 360 / t."""
+    import torch
+
+    from pyronn_layers import geometry, ops, phantoms
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    c = FAN2D
+    g = geometry.FanBeam2D(c["volume"], (c["pixel_mm"],) * 2, c["detector"], c["det_mm"], c["views"], c["sid_mm"],
+                           c["sdd_mm"])
+    vols = np.stack([phantoms.ellipse_phantom_2d(c["volume"], (c["pixel_mm"],) * 2, seed=100 + b)[0]
+                     for b in range(c["batch"])])
+    storage = {"bf16": torch.bfloat16, "fp16": torch.float16, "fp32": torch.float32}[args.storage]
+    units = c["batch"] * c["volume"][0] * c["volume"][1] * c["views"]
+
+    def run(store):
+        x = torch.from_numpy(vols).to(dev, store)
+        geo = ops.Geometry2D(c["batch"], dev, *g.args()[:4], g.ray_vectors, c["views"], g.sid, g.sdd)
+        sino = torch.empty((c["batch"], c["views"], c["detector"]), dtype=store, device=dev)
+        back = torch.empty((c["batch"],) + c["volume"], dtype=torch.float32, device=dev)
+        code = ops.storage_code(store)
+        lib = ops._capi
+        ev = []
+
+        def step():
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            s = torch.cuda.current_stream(dev).cuda_stream
+            e[0].record()
+            lib.call("pyronn_fan_projection2d", x.data_ptr(), sino.data_ptr(), code, code, c["batch"],
+                     *c["volume"], c["views"], c["detector"], *geo.pointers(), geo.g, s)
+            e[1].record()
+            lib.call("pyronn_fan_backprojection2d", sino.data_ptr(), back.data_ptr(), code, 0, c["batch"],
+                     c["views"], c["detector"], *c["volume"], *geo.pointers(), geo.g, s)
+            e[2].record()
+            ev.append(e)
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        ev.clear()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(args.steps):
+            step()
+        t1.record()
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1)
+        f = statistics.mean(a.elapsed_time(b) for a, b, _ in ev)
+        bk = statistics.mean(b.elapsed_time(c2) for _, b, c2 in ev)
+        return 2 * units * args.steps / (ms / 1e3) / 1e9, ms, f, bk, sino, back
+
+    with ClockSampler(physical_gpu_index(dev.index or 0)) as clk:
+        gups, ms, f_ms, b_ms, sino, back = run(storage)
+    gups32 = run(torch.float32)[0] if storage != torch.float32 else None
+    line = {
+        "metric": METRIC, "value": gups, "unit": "GUPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "storage": args.storage, "data": "synthetic",
+        "config": {"workload": "fan2d", "batch": c["batch"], "slice": list(c["volume"]), "pixel_mm": c["pixel_mm"],
+                   "views": c["views"], "detector_px": c["detector"], "det_mm": c["det_mm"], "sid_mm": c["sid_mm"],
+                   "sdd_mm": c["sdd_mm"], "phantom": "10 seeded ellipses per slice"},
+        "plain_fp32_value": gups32,
+        "kernels": {"forward_ms": f_ms, "backprojection_ms": b_ms},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving"], default="cone512")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving", "fan2d"], default="cone512")
     ap.add_argument("--requests", type=int, default=2000, help="serving: number of requests")
     ap.add_argument("--rate", type=float, default=100.0, help="serving: Poisson arrival rate (1/s)")
     ap.add_argument("--storage", choices=["bf16", "fp16", "fp32"], default="bf16")
@@ -513,6 +589,12 @@ def main(argv=None):
                     help="dram bytes per launch of the dominant kernel from an ncu capture")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)  # at least 3 untimed warm-up steps
+    if args.workload == "fan2d":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the fan2d workload is measured on the GPU arm only"}))
+            return
+        run_fan2d(args)
+        return
     if args.workload == "serving":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the serving stream has no CPU reference arm"}))

@@ -335,7 +335,7 @@ int pyronn_cone_projection3d(const void *volume, void *sinogram, int in_dtype, i
             void *scratch = (char *)workspace + WS_HEADER +
                             align_up((size_t)geom_batch * n_proj * sizeof(ConeFpView), 256);
             e = launch_cone_fp_padded(volume, sinogram, in_dtype, out_dtype, d, views, step_size, volume_spacing,
-                                      scratch, s);
+                                      scratch, (unsigned *)workspace, s);
         } else {
             e = launch_cone_fp(volume, sinogram, in_dtype, out_dtype, d, -1, views, step_size, volume_spacing, 0, s);
         }

@@ -3,16 +3,21 @@
 //
 // The reference gathers the 8 trilinear taps straight from the x-fastest
 // volume with a bounds test per tap (cone_projector_3D_CudaKernel.cu.cc:42-85).
-// A warp here is 32 rays of one detector row; at a given step their samples
-// lie on a line perpendicular to the rays.  When the rays run mostly along x
-// that line runs along y, so in an x-fastest layout every lane hits its own
-// cache line.  The call therefore stages two copies of the volume in the
-// workspace, both with a zero border (1 voxel below, 2 above, so the taps of
-// any sample inside the box [0, N] need no bounds test):
-//   * x-fastest [Z+3][Y+3][X+3]  -- used by views whose rays run mostly along y
-//   * y-fastest [Z+3][X+3][Y+3]  -- used by views whose rays run mostly along x
-// Sample positions, weights and the march are those of cone_fp.cu (FP64 ray
-// set-up, FP32 alpha advanced as the reference does), so results are the same.
+// What makes a gather cheap is that the 32 samples a warp takes at one step
+// fall on few cache lines.  Rays of one detector COLUMN (fixed u, varying v)
+// sample at nearly the same (x, y) and at consecutive z whenever the
+// detector's v axis runs along z -- true for every view of a circular
+// trajectory.  Such views ("z mode") lay warps along v and read a z-fastest
+// copy that stores the tap PAIR (V(z), V(z+1)) in each element, so a sample is
+// four pair loads whose warp-wide footprint is a few sectors.
+// Other views ("xy mode") lay warps along u and read an x-fastest or a
+// y-fastest copy, whichever fastest axis runs across their rays.
+// All copies carry a zero border (one voxel below, two above in x, y, z), so
+// the taps of any sample inside the box [0, N] need no bounds test; they are
+// written into the workspace per batch element, and a copy no view needs is
+// skipped on the device.  Sample positions, weights and the march are those
+// of cone_ray.cuh (FP64 ray set-up, FP32 alpha advanced as the reference
+// does), so results match the direct path.
 #include <math_constants.h>
 
 #include "common.cuh"
@@ -27,12 +32,105 @@ constexpr int PB_X = 32;
 constexpr int PB_Y = 8;
 constexpr int PAD_TILE = 32;
 
+// workspace header words (after the error flag) set by classify_views_kernel
+enum { FLAG_NEED_XY = 1, FLAG_NEED_Z = 2 };
+
+// Z-mode test of a view: the ray direction's derivative along detector v,
+// inv_ar (0, 1, 0) in voxel-index space, points along z.
+__device__ __forceinline__ bool view_is_z_mode(const ConeFpView &v)
+{
+    const double cx = v.inv_ar[1], cy = v.inv_ar[4], cz = v.inv_ar[7];
+    return cz * cz >= 0.81 * (cx * cx + cy * cy + cz * cz);
+}
+
+__global__ void classify_views_kernel(const ConeFpView *__restrict__ views, int n, unsigned *__restrict__ flags)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    atomicOr(&flags[view_is_z_mode(views[t]) ? FLAG_NEED_Z : FLAG_NEED_XY], 1u);
+}
+
+// (V(z), V(z+1)) tap pairs: a float2 for FP32, a 32-bit word of two 16-bit
+// values for BF16 / FP16 (the lower-addressed value in the low half)
+template <typename T>
+struct TapPair;
+template <>
+struct TapPair<float> {
+    using type = float2;
+    __device__ static float2 make(float a, float b) { return make_float2(a, b); }
+    __device__ static void unpack(const float2 &w, float &lo, float &hi)
+    {
+        lo = w.x;
+        hi = w.y;
+    }
+};
+template <>
+struct TapPair<__nv_bfloat16> {
+    using type = unsigned;
+    __device__ static unsigned make(__nv_bfloat16 a, __nv_bfloat16 b)
+    {
+        return (unsigned)__bfloat16_as_ushort(a) | ((unsigned)__bfloat16_as_ushort(b) << 16);
+    }
+    __device__ static void unpack(unsigned w, float &lo, float &hi)
+    {
+        lo = __uint_as_float(w << 16);
+        hi = __uint_as_float(w & 0xFFFF0000u);
+    }
+};
+template <>
+struct TapPair<__half> {
+    using type = unsigned;
+    __device__ static unsigned make(__half a, __half b)
+    {
+        return (unsigned)__half_as_ushort(a) | ((unsigned)__half_as_ushort(b) << 16);
+    }
+    __device__ static void unpack(unsigned w, float &lo, float &hi)
+    {
+        lo = __half2float(__ushort_as_half((unsigned short)(w & 0xFFFFu)));
+        hi = __half2float(__ushort_as_half((unsigned short)(w >> 16)));
+    }
+};
+
+// z-fastest pair copy: element [xp][yp][zq] = (V(xp-1, yp-1, zq-1), V(xp-1, yp-1, zq)),
+// xp in [0, X+2], yp in [0, Y+2], zq in [0, Z+1], V zero outside the volume.
+// Reads run along x, writes along z: a 32 x 33 tile is transposed through
+// shared memory.  Skipped when no view is in z mode.
+template <typename T>
+__global__ void __launch_bounds__(PAD_TILE *8) pad_zpairs_kernel(const T *__restrict__ src,
+                                                                  typename TapPair<T>::type *__restrict__ dst, int X,
+                                                                  int Y, int Z, const unsigned *__restrict__ flags)
+{
+    if (!flags[FLAG_NEED_Z]) return;
+    __shared__ T tile[PAD_TILE + 1][PAD_TILE + 1];  // [z][x]
+    const int Yp = Y + 3, Zq = Z + 2;
+    const int xp0 = blockIdx.x * PAD_TILE, yp = blockIdx.y, zq0 = blockIdx.z * PAD_TILE;
+    const int y = yp - 1;
+    const bool yin = y >= 0 && y < Y;
+    for (int r = threadIdx.y; r < PAD_TILE + 1; r += 8) {
+        const int z = zq0 - 1 + r, x = xp0 - 1 + threadIdx.x;
+        T v = T(0.0f);
+        if (yin && z >= 0 && z < Z && x >= 0 && x < X) v = src[((size_t)z * Y + y) * X + x];
+        tile[r][threadIdx.x] = v;
+    }
+    __syncthreads();
+    const int zq = zq0 + threadIdx.x;
+    if (zq < Zq) {
+        for (int c = threadIdx.y; c < PAD_TILE; c += 8) {
+            const int xp = xp0 + c;
+            if (xp < X + 3)
+                dst[((size_t)xp * Yp + yp) * Zq + zq] = TapPair<T>::make(tile[threadIdx.x][c], tile[threadIdx.x + 1][c]);
+        }
+    }
+}
+
 // copies one batch element into both padded layouts; the border is written as
 // zeros by the same kernel (every padded element is written exactly once)
 template <typename T>
 __global__ void __launch_bounds__(PAD_TILE *8) pad_volume_kernel(const T *__restrict__ src, T *__restrict__ xfast,
-                                                                 T *__restrict__ yfast, int X, int Y, int Z)
+                                                                 T *__restrict__ yfast, int X, int Y, int Z,
+                                                                 const unsigned *__restrict__ flags)
 {
+    if (!flags[FLAG_NEED_XY]) return;
     __shared__ T tile[PAD_TILE][PAD_TILE + 1];
     const int Xp = X + 3, Yp = Y + 3;
     const int zp = blockIdx.z;   // padded z
@@ -162,58 +260,139 @@ __device__ __forceinline__ bool march_inside(const ConeRay &r, int X, int Y, int
            fmaxf(y0, y1) <= Y + 0.5f && fmaxf(z0, z1) <= Z + 0.5f;
 }
 
+// Trilinear interpolation from the z-fastest pair copy: four pair loads, one
+// per (x, y) corner, each giving the two z taps.  `origin` points at the
+// element of source voxel (0, 0, 0)'s pair.
+template <typename T>
+struct PairSampler {
+    const typename TapPair<T>::type *origin;
+    int s_y, s_x;  // element strides of y and x (z is fastest)
+
+    __device__ __forceinline__ float operator()(float x, float y, float z) const
+    {
+        const FloorFrac fx = floor_frac(x), fy = floor_frac(y), fz = floor_frac(z);
+        const typename TapPair<T>::type *p = origin + (fx.i * s_x + fy.i * s_y + fz.i);
+        const typename TapPair<T>::type w00 = __ldg(p), w01 = __ldg(p + s_y), w10 = __ldg(p + s_x),
+                                        w11 = __ldg(p + s_x + s_y);
+        float a0, a1, b0, b1, c0, c1, d0, d1;
+        TapPair<T>::unpack(w00, a0, a1);  // (x0, y0)
+        TapPair<T>::unpack(w01, b0, b1);  // (x0, y1)
+        TapPair<T>::unpack(w10, c0, c1);  // (x1, y0)
+        TapPair<T>::unpack(w11, d0, d1);  // (x1, y1)
+        // the reference's order: lerp in z, then y, then x
+        const float z00 = lerp_ref(a0, a1, fz.f), z01 = lerp_ref(b0, b1, fz.f);
+        const float z10 = lerp_ref(c0, c1, fz.f), z11 = lerp_ref(d0, d1, fz.f);
+        return lerp_ref(lerp_ref(z00, z01, fy.f), lerp_ref(z10, z11, fy.f), fx.f);
+    }
+};
+
+template <typename T>
+struct ClampedPairSampler {
+    PairSampler<T> s;
+    float xmax, ymax, zmax;
+    __device__ __forceinline__ float operator()(float x, float y, float z) const
+    {
+        return s(fminf(fmaxf(x, -1.0f), xmax), fminf(fmaxf(y, -1.0f), ymax), fminf(fmaxf(z, -1.0f), zmax));
+    }
+};
+
+// Grid: (ceil(W/32), ceil(H/32), n_proj * 4); each 32 x 32 ray tile is four
+// blocks of 256 threads.  z mode: a warp is 32 consecutive v at one u, and the
+// block's 8 x 32 results go through shared memory so the sinogram rows are
+// written 8 pixels at a time; xy mode: a warp is 32 consecutive u.
 template <typename T, typename Tout>
 __global__ void __launch_bounds__(PB_X *PB_Y)
-    cone_fp_padded_kernel(const T *__restrict__ xfast, const T *__restrict__ yfast, Tout *__restrict__ sino,
+    cone_fp_padded_kernel(const T *__restrict__ xfast, const T *__restrict__ yfast,
+                          const typename TapPair<T>::type *__restrict__ zpairs, Tout *__restrict__ sino,
                           const ConeFpView *__restrict__ views, const float *__restrict__ step_ptr,
                           const float *__restrict__ spacing_ptr, int X, int Y, int Z, int W, int H, int n_proj,
                           int geom_batch, int b)
 {
-    const int u = blockIdx.x * PB_X + threadIdx.x;
-    const int v = blockIdx.y * PB_Y + threadIdx.y;
-    const int p = blockIdx.z;
-    if (u >= W || v >= H) return;
+    __shared__ float out_tile[PB_Y][PB_X + 1];
+    const int p = blockIdx.z >> 2, sub = blockIdx.z & 3;
     const int g = geom_batch == 1 ? 0 : b;
     const ConeFpView &view = views[(size_t)g * n_proj + p];
-    const float step = step_ptr[g];
-    const ConeRay ray = cone_ray_setup(view, u, v, X, Y, Z, 0.0, step, spacing_ptr[g * 3 + 2], spacing_ptr[g * 3 + 1],
-                                       spacing_ptr[g * 3 + 0]);
-    // layout of this view (uniform per block): rays mostly along x -> y-fastest copy
-    const double cr0 = view.inv_ar[2] + 0.5 * (W - 1) * view.inv_ar[0] + 0.5 * (H - 1) * view.inv_ar[1];
-    const double cr1 = view.inv_ar[5] + 0.5 * (W - 1) * view.inv_ar[3] + 0.5 * (H - 1) * view.inv_ar[4];
-    const bool along_x = fabs(cr0) > fabs(cr1);
-    const int Xp = X + 3, Yp = Y + 3;
-    const int s_slice = Xp * Yp;
-    const bool inside = march_inside(ray, X, Y, Z);
-    const float xmax = (float)X + 0.999f, ymax = (float)Y + 0.999f, zmax = (float)Z + 0.999f;
-    float pixel;
-    if (along_x) {
-        const PaddedSampler<T, true> s{yfast + s_slice + Yp + 1, Yp, s_slice};
-        pixel = inside ? march_x2(ray, step, s) : march_x2(ray, step, ClampedSampler<T, true>{s, xmax, ymax, zmax});
+    const bool zmode = view_is_z_mode(view);
+    int u, v;
+    if (zmode) {
+        u = blockIdx.x * 32 + sub * PB_Y + threadIdx.y;
+        v = blockIdx.y * 32 + threadIdx.x;
     } else {
-        const PaddedSampler<T, false> s{xfast + s_slice + Xp + 1, Xp, s_slice};
-        pixel = inside ? march_x2(ray, step, s) : march_x2(ray, step, ClampedSampler<T, false>{s, xmax, ymax, zmax});
+        u = blockIdx.x * 32 + threadIdx.x;
+        v = blockIdx.y * 32 + sub * PB_Y + threadIdx.y;
     }
-    store_from_float(sino + (((size_t)b * n_proj + p) * H + v) * (size_t)W + u, pixel);
+    const bool live = u < W && v < H;
+    const float step = step_ptr[g];
+    float pixel = 0.0f;
+    if (live) {
+        const ConeRay ray = cone_ray_setup(view, u, v, X, Y, Z, 0.0, step, spacing_ptr[g * 3 + 2],
+                                           spacing_ptr[g * 3 + 1], spacing_ptr[g * 3 + 0]);
+        const bool inside = march_inside(ray, X, Y, Z);
+        const float xmax = (float)X + 0.999f, ymax = (float)Y + 0.999f, zmax = (float)Z + 0.999f;
+        const int Xp = X + 3, Yp = Y + 3;
+        if (zmode) {
+            const int Zq = Z + 2;
+            const PairSampler<T> s{zpairs + (Yp + 1) * Zq + 1, Zq, Yp * Zq};
+            pixel = inside ? march_x2(ray, step, s) : march_x2(ray, step, ClampedPairSampler<T>{s, xmax, ymax, zmax});
+        } else {
+            // rays mostly along x -> y-fastest copy
+            const double cr0 = view.inv_ar[2] + 0.5 * (W - 1) * view.inv_ar[0] + 0.5 * (H - 1) * view.inv_ar[1];
+            const double cr1 = view.inv_ar[5] + 0.5 * (W - 1) * view.inv_ar[3] + 0.5 * (H - 1) * view.inv_ar[4];
+            const int s_slice = Xp * Yp;
+            if (fabs(cr0) > fabs(cr1)) {
+                const PaddedSampler<T, true> s{yfast + s_slice + Yp + 1, Yp, s_slice};
+                pixel = inside ? march_x2(ray, step, s)
+                               : march_x2(ray, step, ClampedSampler<T, true>{s, xmax, ymax, zmax});
+            } else {
+                const PaddedSampler<T, false> s{xfast + s_slice + Xp + 1, Xp, s_slice};
+                pixel = inside ? march_x2(ray, step, s)
+                               : march_x2(ray, step, ClampedSampler<T, false>{s, xmax, ymax, zmax});
+            }
+        }
+    }
+    Tout *out = sino + ((size_t)b * n_proj + p) * H * (size_t)W;
+    if (!zmode) {
+        if (live) store_from_float(out + (size_t)v * W + u, pixel);
+        return;
+    }
+    // z mode: transpose the 8 (u) x 32 (v) results so each row is written as 8 pixels
+    out_tile[threadIdx.y][threadIdx.x] = pixel;
+    __syncthreads();
+    const int t = threadIdx.y * PB_X + threadIdx.x;
+    const int ov = blockIdx.y * 32 + t / PB_Y, ou = blockIdx.x * 32 + sub * PB_Y + t % PB_Y;
+    if (ov < H && ou < W) store_from_float(out + (size_t)ov * W + ou, out_tile[t % PB_Y][t / PB_Y]);
+}
+
+size_t section_bytes(size_t n)
+{
+    return (n + 255) / 256 * 256;
 }
 
 template <typename Tin, typename Tout>
 cudaError_t launch_typed(const void *volume, void *sinogram, const Dims3D &d, const ConeFpView *views,
-                         const float *step, const float *spacing, void *scratch, cudaStream_t stream)
+                         const float *step, const float *spacing, void *scratch, unsigned *flags, cudaStream_t stream)
 {
-    const size_t padded = (size_t)(d.vol_x + 3) * (d.vol_y + 3) * (d.vol_z + 3);
-    Tin *xfast = (Tin *)scratch;
-    Tin *yfast = xfast + padded;
+    using Pair = typename TapPair<Tin>::type;
+    const size_t Xp = d.vol_x + 3, Yp = d.vol_y + 3, Zp = d.vol_z + 3, Zq = d.vol_z + 2;
+    char *base = (char *)scratch;
+    Tin *xfast = (Tin *)base;
+    Tin *yfast = (Tin *)(base + section_bytes(Xp * Yp * Zp * sizeof(Tin)));
+    Pair *zpairs = (Pair *)(base + 2 * section_bytes(Xp * Yp * Zp * sizeof(Tin)));
+    const int nviews = d.geom_batch * d.n_proj;
+    classify_views_kernel<<<(nviews + 127) / 128, 128, 0, stream>>>(views, nviews, flags);
     const dim3 pblock(PAD_TILE, 8);
-    const dim3 pgrid((d.vol_x + 3 + PAD_TILE - 1) / PAD_TILE, (d.vol_y + 3 + PAD_TILE - 1) / PAD_TILE, d.vol_z + 3);
+    const dim3 pgrid((unsigned)((Xp + PAD_TILE - 1) / PAD_TILE), (unsigned)((Yp + PAD_TILE - 1) / PAD_TILE),
+                     (unsigned)Zp);
+    const dim3 zgrid((unsigned)((Xp + PAD_TILE - 1) / PAD_TILE), (unsigned)Yp, (unsigned)((Zq + PAD_TILE - 1) / PAD_TILE));
     const dim3 block(PB_X, PB_Y);
-    const dim3 grid((d.det_w + PB_X - 1) / PB_X, (d.det_h + PB_Y - 1) / PB_Y, d.n_proj);
+    const dim3 grid((d.det_w + 31) / 32, (d.det_h + 31) / 32, d.n_proj * 4);
     for (int b = 0; b < d.batch; ++b) {
         const Tin *src = (const Tin *)volume + (size_t)b * d.vol_z * d.vol_y * d.vol_x;
-        pad_volume_kernel<Tin><<<pgrid, pblock, 0, stream>>>(src, xfast, yfast, d.vol_x, d.vol_y, d.vol_z);
-        cone_fp_padded_kernel<Tin, Tout><<<grid, block, 0, stream>>>(xfast, yfast, (Tout *)sinogram, views, step,
-                                                                     spacing, d.vol_x, d.vol_y, d.vol_z, d.det_w,
-                                                                     d.det_h, d.n_proj, d.geom_batch, b);
+        pad_volume_kernel<Tin><<<pgrid, pblock, 0, stream>>>(src, xfast, yfast, d.vol_x, d.vol_y, d.vol_z, flags);
+        pad_zpairs_kernel<Tin><<<zgrid, pblock, 0, stream>>>(src, zpairs, d.vol_x, d.vol_y, d.vol_z, flags);
+        cone_fp_padded_kernel<Tin, Tout><<<grid, block, 0, stream>>>(xfast, yfast, zpairs, (Tout *)sinogram, views,
+                                                                     step, spacing, d.vol_x, d.vol_y, d.vol_z,
+                                                                     d.det_w, d.det_h, d.n_proj, d.geom_batch, b);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
@@ -224,23 +403,26 @@ cudaError_t launch_typed(const void *volume, void *sinogram, const Dims3D &d, co
 
 size_t cone_fp_padded_scratch_bytes(int vol_z, int vol_y, int vol_x, int in_dtype)
 {
-    return 2 * (size_t)(vol_x + 3) * (vol_y + 3) * (vol_z + 3) * dtype_size(in_dtype);
+    const size_t e = dtype_size(in_dtype);
+    const size_t plane = (size_t)(vol_x + 3) * (vol_y + 3);
+    return 2 * section_bytes(plane * (vol_z + 3) * e) + section_bytes(plane * (vol_z + 2) * 2 * e);
 }
 
 bool cone_fp_padded_supported(const Dims3D &d)
 {
     const long long padded = (long long)(d.vol_x + 3) * (d.vol_y + 3) * (d.vol_z + 3);
-    return padded < (1LL << 31) - (1LL << 20) && d.n_proj <= 65535 && d.vol_z + 3 <= 65535;
+    return padded < (1LL << 31) - (1LL << 20) && (long long)d.n_proj * 4 <= 65535 && d.vol_z + 3 <= 65535 &&
+           d.vol_y + 3 <= 65535;
 }
 
 cudaError_t launch_cone_fp_padded(const void *volume, void *sinogram, int in_dtype, int out_dtype, const Dims3D &d,
                                   const ConeFpView *views, const float *step, const float *spacing, void *scratch,
-                                  cudaStream_t stream)
+                                  unsigned *flags, cudaStream_t stream)
 {
     return dispatch_dtypes(in_dtype, out_dtype, [&](auto tin, auto tout) {
         using Tin = typename decltype(tin)::type;
         using Tout = typename decltype(tout)::type;
-        return launch_typed<Tin, Tout>(volume, sinogram, d, views, step, spacing, scratch, stream);
+        return launch_typed<Tin, Tout>(volume, sinogram, d, views, step, spacing, scratch, flags, stream);
     });
 }
 

@@ -59,9 +59,10 @@ cudaError_t launch_cone_bp(const void *sinogram, void *volume, int in_dtype, int
 // software forward projector over padded, view-oriented copies (cone_fp_padded.cu)
 size_t cone_fp_padded_scratch_bytes(int vol_z, int vol_y, int vol_x, int in_dtype);
 bool cone_fp_padded_supported(const Dims3D &d);
+// flags: zeroed header words of the workspace (the kernel records which copies it needs)
 cudaError_t launch_cone_fp_padded(const void *volume, void *sinogram, int in_dtype, int out_dtype, const Dims3D &d,
                                   const ConeFpView *views, const float *step, const float *spacing, void *scratch,
-                                  cudaStream_t stream);
+                                  unsigned *flags, cudaStream_t stream);
 
 // matched (exact-adjoint) scatter backprojector (cone_matched.cu); FP32 output
 cudaError_t launch_cone_scatter(const void *sinogram, float *volume, int in_dtype, const Dims3D &d,

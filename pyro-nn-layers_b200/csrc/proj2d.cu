@@ -28,9 +28,10 @@ constexpr int BP2_BLOCK_Y = 8;
 template <typename T>
 __device__ __forceinline__ float interp2d_border(const T *__restrict__ img, float x, float y, int X, int Y)
 {
-    const float fx = floorf(x), fy = floorf(y);
-    const int x0 = __float2int_rz(fx), y0 = __float2int_rz(fy);
-    const float tx = x - fx, ty = y - fy;
+    // sample positions stay inside the box (|x|, |y| << 2^22): exact FADD floor
+    const FloorFrac ffx = floor_frac(x), ffy = floor_frac(y);
+    const int x0 = ffx.i, y0 = ffy.i;
+    const float tx = ffx.f, ty = ffy.f;
     const bool vx0 = (unsigned)x0 < (unsigned)X, vx1 = (unsigned)(x0 + 1) < (unsigned)X;
     const bool vy0 = (unsigned)y0 < (unsigned)Y, vy1 = (unsigned)(y0 + 1) < (unsigned)Y;
     const int base = y0 * X + x0;
@@ -118,12 +119,27 @@ __global__ void __launch_bounds__(FP2_BLOCK)
             a += step;
             ++iter;
         }
+        // two samples per iteration (their gathers overlap); same alpha
+        // sequence and the same order of additions as one at a time
         while (a < am && iter < max_iter) {
-            px = fmaf(a, gx, bx);
-            py = fmaf(a, gy, by);
-            pixel += interp2d_border<T>(img, px, py, X, Y);
-            a += step;
-            ++iter;
+            const float a1 = a + step;
+            if (a1 < am && iter + 1 < max_iter) {
+                const float qx = fmaf(a, gx, bx), qy = fmaf(a, gy, by);
+                px = fmaf(a1, gx, bx);
+                py = fmaf(a1, gy, by);
+                const float v0 = interp2d_border<T>(img, qx, qy, X, Y);
+                const float v1 = interp2d_border<T>(img, px, py, X, Y);
+                pixel += v0;
+                pixel += v1;
+                a = a1 + step;
+                iter += 2;
+            } else {
+                px = fmaf(a, gx, bx);
+                py = fmaf(a, gy, by);
+                pixel += interp2d_border<T>(img, px, py, X, Y);
+                a += step;
+                ++iter;
+            }
         }
         pixel *= step;
         if (pixel > 0.0f) {  // :88-100

@@ -48,11 +48,12 @@ def test_workspace_sizes():
     fp16 = lib.pyronn_cone_projection3d_workspace_size(2, 64, 64, 64, 360, 100, 120, 1, 0, 2)
     bp = lib.pyronn_cone_backprojection3d_workspace_size(2, 360, 100, 120, 64, 64, 64, 0, 0, 2)
     assert fp_hw >= 256 + 2 * 360 * 96 and fp_hw % 256 == 0
-    # two zero-padded copies of one volume for the software forward path
+    # zero-padded copies of one volume for the software forward path: x- and
+    # y-fastest (67^3 each) and the z-fastest tap-pair copy (67 x 67 x 66 pairs)
     def align(n):
         return (n + 255) // 256 * 256
-    assert fp - fp_hw == align(2 * 67 ** 3 * 4)
-    assert fp16 - fp_hw == align(2 * 67 ** 3 * 2)
+    assert fp - fp_hw == 2 * align(67 ** 3 * 4) + align(67 * 67 * 66 * 8)
+    assert fp16 - fp_hw == 2 * align(67 ** 3 * 2) + align(67 * 67 * 66 * 4)
     assert bp >= 256 + 2 * 360 * 48 and bp % 256 == 0
     assert lib.pyronn_cone_projection3d_workspace_size(0, 8, 8, 8, 10, 4, 4, 0, 0, 1) == 0
     assert lib.pyronn_cone_projection3d_workspace_size(1, 8, 8, 8, 10, 4, 4, 9, 0, 1) == 0

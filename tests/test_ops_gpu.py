@@ -359,3 +359,19 @@ def test_unrolled_reconstruction_with_checkpointing(cuda):
         loss0 = 0.5 * ((pl.cone_projection3d(x0, geo.detector_shape, *geo.args()) - y) ** 2).sum()
         assert float(loss) < float(loss0)
     torch.testing.assert_close(grads[0], grads[1], rtol=1e-5, atol=0)
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.bfloat16])
+def test_cone_projection_non_circular_views(cuda, dtype):
+    """Views whose detector v axis is not along z (a trajectory about the y
+    axis: P's y and z columns swapped) take the forward projector's xy mode;
+    mixing them with circular views exercises both modes in one launch."""
+    geo = _cone_geo(n_proj=12)
+    P = np.asarray(geo.projection_matrices).copy()
+    P[::2] = P[::2][:, :, [0, 2, 1, 3]]  # every other view rotates about y
+    args = (geo.volume_origin, geo.volume_spacing, P, geo.step_size, geo.projection_multiplier)
+    vol = phantoms.ellipsoid_phantom_3d(geo.volume_shape, geo.volume_spacing, seed=9, n=6)[0][None]
+    x = t(vol, cuda, dtype)
+    out = pl.cone_projection3d(x, geo.detector_shape, *args, out_dtype=torch.float32)
+    ref = oracle.cone_projection3d(rounded(x), geo.detector_shape, *args)
+    assert rel_l2(out.cpu().numpy(), ref) < 2e-5
