@@ -256,17 +256,22 @@ def run_reference(args, cfg):
     print(json.dumps(line))
 
 
+def sino_storage_name(args):
+    return args.storage if args.sino_storage == "same" else args.sino_storage
+
+
 def config_block(args, cfg):
     z, y, x = cfg["volume"]
     return {"workload": args.workload, "volume": list(cfg["volume"]), "voxel_mm": cfg["voxel_mm"],
             "views": cfg["views"], "detector_hw": list(cfg["detector"]), "pixel_mm": cfg["pixel_mm"],
             "sid_mm": cfg["sid_mm"], "sdd_mm": cfg["sdd_mm"], "step_voxels": cfg["step_voxels"],
             "hardware_interp": bool(args.hardware_interp), "storage": args.storage,
+            "sinogram_storage": sino_storage_name(args),
             "updates_per_op": updates(cfg), "phantom": "%d seeded ellipsoids" % PHANTOM_ELLIPSOIDS,
             "l2": "inputs larger than L2 (volume %d MB, sinogram %d MB at the storage dtype)"
                   % (z * y * x * (4 if args.storage == "fp32" else 2) >> 20,
-                     cfg["views"] * cfg["detector"][0] * cfg["detector"][1] * (4 if args.storage == "fp32" else 2)
-                     >> 20),
+                     cfg["views"] * cfg["detector"][0] * cfg["detector"][1]
+                     * (4 if sino_storage_name(args) == "fp32" else 2) >> 20),
             "parallelism": "replicas (one volume per GPU)" if args.gpus > 1 else "single GPU"}
 
 
@@ -288,7 +293,9 @@ def run_ours(args, cfg):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
     dev = torch.device("cuda", local_rank)
-    storage = {"bf16": torch.bfloat16, "fp16": torch.float16, "fp32": torch.float32}[args.storage]
+    dtypes = {"bf16": torch.bfloat16, "fp16": torch.float16, "fp32": torch.float32}
+    storage = dtypes[args.storage]
+    sino_storage = dtypes[sino_storage_name(args)]
 
     geo = geometry.ConeBeam3D(cfg["volume"], (cfg["voxel_mm"],) * 3, cfg["detector"], (cfg["pixel_mm"],) * 2,
                               cfg["views"], cfg["sid_mm"], cfg["sdd_mm"], step_size=cfg["step_voxels"])
@@ -363,9 +370,9 @@ def run_ours(args, cfg):
             ms = float(t.item())
         return ms
 
-    # ---- the headline configuration (storage dtype in, FP32 volume out)
-    out_fwd = storage
-    step, ev, x, sino, back = make_step(storage, out_fwd, torch.float32)
+    # ---- the headline configuration (storage dtype in, sinogram storage
+    # between the ops, FP32 volume out)
+    step, ev, x, sino, back = make_step(storage, sino_storage, torch.float32)
     with ClockSampler(physical_gpu_index(local_rank)) as clk:
         ms = timed(lambda rec=False: step(rec), args.steps, args.warmup, True)
     clocks = clk.summary()
@@ -390,7 +397,7 @@ def run_ours(args, cfg):
 
     def e2e_step(rec=False):
         xd = host_in.to(dev, non_blocking=True)
-        s = pl.cone_projection3d(xd, geo.detector_shape, *args_geo, hardware_interp=hw)
+        s = pl.cone_projection3d(xd, geo.detector_shape, *args_geo, hardware_interp=hw, out_dtype=sino_storage)
         b = pl.cone_backprojection3d(s, geo.volume_shape, *args_geo, hardware_interp=hw, out_dtype=torch.float32)
         host_out.copy_(b, non_blocking=True)
 
@@ -400,10 +407,11 @@ def run_ours(args, cfg):
 
     # ---- roofline of the dominant kernel
     es = 2 if storage != torch.float32 else 4
+    es_s = 2 if sino_storage != torch.float32 else 4
     S = count_samples(cfg, dev)
     f_ms, b_ms = statistics.mean(fwd_ms), statistics.mean(back_ms)
-    fwd_bytes = S * 8 * es + n_proj * H * W * es
-    back_bytes = updates(cfg) * 4 * es + Z * Y * X * 4
+    fwd_bytes = S * 8 * es + n_proj * H * W * es_s
+    back_bytes = updates(cfg) * 4 * es_s + Z * Y * X * 4
     peak, peak_kind = measured_peaks()
     if f_ms >= b_ms:
         dom, dom_bytes, dom_ms = "cone_fp_kernel (forward)", fwd_bytes, f_ms
@@ -421,7 +429,8 @@ def run_ours(args, cfg):
     line = {
         "metric": METRIC, "value": value, "unit": "GUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "storage": args.storage, "data": "synthetic",
+        "vs_baseline": None, "dtype": "f32", "storage": args.storage,
+        "sinogram_storage": sino_storage_name(args), "data": "synthetic",
         "config": config_block(args, cfg),
         "plain_fp32_value": fp32_gups,
         "storage_over_fp32": (value / fp32_gups) if fp32_gups else None,
@@ -451,9 +460,9 @@ def run_ours(args, cfg):
         line["accuracy"] = {
             "forward_rel_l2_vs_fp64": rel(ours_f, outs["fwd"]),
             "backprojection_rel_l2_vs_fp64": rel(ours_b, outs["back"]),
-            "note": "forward: %s storage of the FP32 phantom and of the sinogram vs the FP64 oracle on the FP32 "
-                    "phantom (%d view); backprojection: same sinogram, FP32 volume, %d z-slices" % (args.storage,
-                                                                                                  nv, ns)}
+            "note": "forward: %s storage of the FP32 phantom, %s sinogram, vs the FP64 oracle on the FP32 "
+                    "phantom (%d view); backprojection: same sinogram, FP32 volume, %d z-slices"
+                    % (args.storage, sino_storage_name(args), nv, ns)}
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
@@ -527,6 +536,8 @@ def run_fan2d(args):
         back = torch.empty((c["batch"],) + c["volume"], dtype=torch.float32, device=dev)
         code = ops.storage_code(store)
         lib = ops._capi
+        ws = torch.empty(lib.workspace_size("pyronn_projection2d", c["batch"], *c["volume"], code),
+                         dtype=torch.uint8, device=dev)
         ev = []
 
         def step():
@@ -534,7 +545,7 @@ def run_fan2d(args):
             s = torch.cuda.current_stream(dev).cuda_stream
             e[0].record()
             lib.call("pyronn_fan_projection2d", x.data_ptr(), sino.data_ptr(), code, code, c["batch"],
-                     *c["volume"], c["views"], c["detector"], *geo.pointers(), geo.g, s)
+                     *c["volume"], c["views"], c["detector"], *geo.pointers(), geo.g, ws.data_ptr(), ws.numel(), s)
             e[1].record()
             lib.call("pyronn_fan_backprojection2d", sino.data_ptr(), back.data_ptr(), code, 0, c["batch"],
                      c["views"], c["detector"], *c["volume"], *geo.pointers(), geo.g, s)
@@ -582,7 +593,12 @@ def main(argv=None):
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving", "fan2d"], default="cone512")
     ap.add_argument("--requests", type=int, default=2000, help="serving: number of requests")
     ap.add_argument("--rate", type=float, default=100.0, help="serving: Poisson arrival rate (1/s)")
-    ap.add_argument("--storage", choices=["bf16", "fp16", "fp32"], default="bf16")
+    ap.add_argument("--storage", choices=["bf16", "fp16", "fp32"], default="fp16",
+                    help="storage of the volume the forward projection reads (fp16: the 16-bit format that keeps "
+                         "the forward within 1e-3 of the FP64 oracle; bf16 rounds piecewise-constant densities "
+                         "to ~1.2e-3)")
+    ap.add_argument("--sino-storage", choices=["same", "bf16", "fp16", "fp32"], default="same",
+                    help="storage of the sinogram between the two ops ('same': as --storage)")
     ap.add_argument("--hardware-interp", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--traffic-bytes", type=float, default=None,

@@ -91,7 +91,16 @@ PYRONN_API int pyronn_parallel_projection2d(const void *volume, void *sinogram, 
                                  int batch, int vol_y, int vol_x, int n_proj, int det_w,
                                  const float *volume_origin, const float *detector_origin,
                                  const float *volume_spacing, const float *detector_spacing,
-                                 const float *ray_vectors, int geom_batch, void *stream);
+                                 const float *ray_vectors, int geom_batch,
+                                 void *workspace, size_t workspace_bytes, void *stream);
+
+/* Workspace bytes of a 2D forward projection (parallel or fan): two copies
+ * of the batch as bilinear cells (the four taps of each cell together, zero
+ * border), one x-fastest and one y-fastest, so that a sample is one load and
+ * a warp's loads stay on few cache lines whatever the view direction.
+ * workspace may also be NULL: the call then reads the caller's volume with a
+ * bounds test per tap (same results, slower). */
+PYRONN_API size_t pyronn_projection2d_workspace_size(int batch, int vol_y, int vol_x, int in_dtype);
 
 /* ---------------------------------------------------------------------------
  * ParallelBackprojection2D
@@ -118,7 +127,8 @@ PYRONN_API int pyronn_fan_projection2d(const void *volume, void *sinogram, int i
                             const float *volume_spacing, const float *detector_spacing,
                             const float *source_2_isocenter_distance,
                             const float *source_2_detector_distance,
-                            const float *central_ray_vectors, int geom_batch, void *stream);
+                            const float *central_ray_vectors, int geom_batch,
+                            void *workspace, size_t workspace_bytes, void *stream);
 
 /* ---------------------------------------------------------------------------
  * FanBackprojection2D

@@ -144,7 +144,7 @@ int check_texture_layered(int w, int h, int layers)
 }
 
 int run_2d(bool forward, bool fan, const void *in, void *out, int in_dtype, int out_dtype, const Dims2D &d,
-           const Geom2D &g, void *stream)
+           const Geom2D &g, void *workspace, size_t workspace_bytes, void *stream)
 {
     const char *name = forward ? (fan ? "fan_projection2d" : "parallel_projection2d")
                                : (fan ? "fan_backprojection2d" : "parallel_backprojection2d");
@@ -162,8 +162,18 @@ int run_2d(bool forward, bool fan, const void *in, void *out, int in_dtype, int 
     if (st) return st;
     st = check_elements(name, (long long)d.n_proj * d.det_w);
     if (st) return st;
+    void *cells = nullptr;
+    if (forward && workspace) {
+        const size_t need = pyronn_projection2d_workspace_size(d.batch, d.vol_y, d.vol_x, in_dtype);
+        if (workspace_bytes < need)
+            return fail(PYRONN_ERROR_WORKSPACE_TOO_SMALL, "%s: workspace of %zu bytes needed, %zu given", name, need,
+                        workspace_bytes);
+        if (((uintptr_t)workspace) % 16 != 0)
+            return fail(PYRONN_ERROR_INVALID_ARGUMENT, "%s: workspace must be 16-byte aligned", name);
+        cells = workspace;
+    }
     cudaStream_t s = (cudaStream_t)stream;
-    cudaError_t e = forward ? launch_projection2d(in, out, in_dtype, out_dtype, fan, d, g, s)
+    cudaError_t e = forward ? launch_projection2d(in, out, in_dtype, out_dtype, fan, d, g, cells, s)
                             : launch_backprojection2d(in, out, in_dtype, out_dtype, fan, d, g, s);
     if (e != cudaSuccess) return cuda_fail(e, name);
     return ok();
@@ -224,14 +234,21 @@ int pyronn_release_cached_arrays(void)
     return ok();
 }
 
+size_t pyronn_projection2d_workspace_size(int batch, int vol_y, int vol_x, int in_dtype)
+{
+    if (batch <= 0 || vol_y <= 0 || vol_x <= 0 || !valid_dtype(in_dtype)) return 0;
+    // two copies of the batch as bilinear cells (4 taps each, zero border)
+    return 2 * align_up((size_t)batch * (vol_y + 2) * (vol_x + 2) * 4 * dtype_size(in_dtype), 256);
+}
+
 int pyronn_parallel_projection2d(const void *volume, void *sinogram, int in_dtype, int out_dtype, int batch, int vol_y, int vol_x,
                                  int n_proj, int det_w, const float *volume_origin, const float *detector_origin,
                                  const float *volume_spacing, const float *detector_spacing, const float *ray_vectors,
-                                 int geom_batch, void *stream)
+                                 int geom_batch, void *workspace, size_t workspace_bytes, void *stream)
 {
     const Dims2D d{batch, vol_y, vol_x, n_proj, det_w, geom_batch};
     const Geom2D g{volume_origin, detector_origin, volume_spacing, detector_spacing, ray_vectors, nullptr, nullptr};
-    return run_2d(true, false, volume, sinogram, in_dtype, out_dtype, d, g, stream);
+    return run_2d(true, false, volume, sinogram, in_dtype, out_dtype, d, g, workspace, workspace_bytes, stream);
 }
 
 int pyronn_parallel_backprojection2d(const void *sinogram, void *volume, int in_dtype, int out_dtype, int batch, int n_proj, int det_w,
@@ -241,19 +258,20 @@ int pyronn_parallel_backprojection2d(const void *sinogram, void *volume, int in_
 {
     const Dims2D d{batch, vol_y, vol_x, n_proj, det_w, geom_batch};
     const Geom2D g{volume_origin, detector_origin, volume_spacing, detector_spacing, ray_vectors, nullptr, nullptr};
-    return run_2d(false, false, sinogram, volume, in_dtype, out_dtype, d, g, stream);
+    return run_2d(false, false, sinogram, volume, in_dtype, out_dtype, d, g, nullptr, 0, stream);
 }
 
 int pyronn_fan_projection2d(const void *volume, void *sinogram, int in_dtype, int out_dtype, int batch, int vol_y, int vol_x,
                             int n_proj, int det_w, const float *volume_origin, const float *detector_origin,
                             const float *volume_spacing, const float *detector_spacing,
                             const float *source_2_isocenter_distance, const float *source_2_detector_distance,
-                            const float *central_ray_vectors, int geom_batch, void *stream)
+                            const float *central_ray_vectors, int geom_batch, void *workspace,
+                            size_t workspace_bytes, void *stream)
 {
     const Dims2D d{batch, vol_y, vol_x, n_proj, det_w, geom_batch};
     const Geom2D g{volume_origin, detector_origin, volume_spacing, detector_spacing, central_ray_vectors,
                    source_2_isocenter_distance, source_2_detector_distance};
-    return run_2d(true, true, volume, sinogram, in_dtype, out_dtype, d, g, stream);
+    return run_2d(true, true, volume, sinogram, in_dtype, out_dtype, d, g, workspace, workspace_bytes, stream);
 }
 
 int pyronn_fan_backprojection2d(const void *sinogram, void *volume, int in_dtype, int out_dtype, int batch, int n_proj, int det_w,
@@ -265,7 +283,7 @@ int pyronn_fan_backprojection2d(const void *sinogram, void *volume, int in_dtype
     const Dims2D d{batch, vol_y, vol_x, n_proj, det_w, geom_batch};
     const Geom2D g{volume_origin, detector_origin, volume_spacing, detector_spacing, central_ray_vectors,
                    source_2_isocenter_distance, source_2_detector_distance};
-    return run_2d(false, true, sinogram, volume, in_dtype, out_dtype, d, g, stream);
+    return run_2d(false, true, sinogram, volume, in_dtype, out_dtype, d, g, nullptr, 0, stream);
 }
 
 size_t pyronn_cone_projection3d_workspace_size(int batch, int vol_z, int vol_y, int vol_x, int n_proj, int det_h,

@@ -88,22 +88,25 @@ cudaError_t dispatch_dtypes(int in_dtype, int out_dtype, F &&f)
 }
 
 // floor and fraction without the conversion pipe: for |x| < 2^22,
-// y = (x - 0.5) + 1.5 * 2^23 rounds to the integer nearest x - 0.5, i.e.
-// floor(x) -- at an exact integer x = k the tie may give k - 1 with
-// frac = 1, which interpolates to exactly the same value (lerp(a, b, 1) == b
-// and lerp(a, b, 0) == a in the FMA form).  The integer is read from y's
-// mantissa.  Four FADDs and an integer add instead of FRND + F2I.
+// y = x + 1.5 * 2^23 rounded toward -inf lies in [2^23, 2^24), where the
+// spacing of floats is 1, so y = 1.5 * 2^23 + floor(x) exactly and floor(x)
+// is y's mantissa.  Three FADDs and an integer subtract instead of
+// FRND + F2I; the fraction x - floor(x) is exact.
+constexpr int FLOOR_BIAS = 0x4B400000;  // bit pattern of 1.5 * 2^23
+
 struct FloorFrac {
-    int i;
-    float f;  // x - i, exact
+    int i;     // floor(x)
+    int bits;  // floor(x) + FLOOR_BIAS: callers that fold the bias elsewhere
+    float f;   // x - floor(x), exact, in [0, 1)
 };
 
 __device__ __forceinline__ FloorFrac floor_frac(float x)
 {
     const float magic = 12582912.0f;  // 1.5 * 2^23
-    const float y = __fadd_rn(__fadd_rn(x, -0.5f), magic);
+    const float y = __fadd_rd(x, magic);
     FloorFrac r;
-    r.i = __float_as_int(y) - 0x4B400000;
+    r.bits = __float_as_int(y);
+    r.i = r.bits - FLOOR_BIAS;
     r.f = __fadd_rn(x, -__fadd_rn(y, -magic));
     return r;
 }

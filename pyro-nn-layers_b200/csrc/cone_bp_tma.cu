@@ -18,6 +18,12 @@
 // not fit the box, or has a corner at w <= 0, is computed from global memory
 // with the reference's tap rules instead.  A (tile, view) whose taps all lie
 // outside the detector contributes zero and is skipped.
+//
+// Views whose u and w rows have a zero z coefficient -- every view of a
+// circular trajectory about the z axis -- take a column loop: 1/w, u, the u
+// tap and its weight are then the same for the thread's 8 voxels and are
+// computed once; the values are exactly those of the general loop, so is the
+// result.
 #include <cuda.h>
 
 #include "common.cuh"
@@ -43,7 +49,8 @@ struct ViewMeta {
     float u0, v0;   // box origin (pixels), as floats
     int iu0, iv0;   // box origin, as ints
     int mode;
-    int pad[3];
+    int zconst;     // row[0].z == row[2].z == 0: u and w constant along z
+    int pad[2];
 };
 
 template <typename T>
@@ -153,6 +160,7 @@ __device__ __forceinline__ void pass_meta(ViewMeta *meta, const ConeBpView *__re
         m.iu0 = iu0;
         m.iv0 = iv0;
         m.mode = mode;
+        m.zconst = (r0.z == 0.0f && r2.z == 0.0f) ? 1 : 0;
         meta[k] = m;
     }
 }
@@ -236,7 +244,30 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
             const float ub = fmaf(r0.x, fi, fmaf(r0.y, fj, fmaf(r0.z, fk, r0.w)));
             const float vb = fmaf(r1.x, fi, fmaf(r1.y, fj, fmaf(r1.z, fk, r1.w)));
             const float wb = fmaf(r2.x, fi, fmaf(r2.y, fj, fmaf(r2.z, fk, r2.w)));
-            if (mode == MODE_SMEM) {
+            if (mode == MODE_SMEM && m.zconst) {
+                const T *tile = &tiles[cur][k][0];
+                // fmaf(0, z, x) == x: these are the general loop's values at every z
+                const float rw = fast_rcp(wb);
+                const FloorFrac fu = floor_frac(ub * rw - m.u0);
+                const float tx = fu.f;
+                // row of floor(lv) from its FloorFrac bits: the bias folded into one offset
+                const unsigned col = (unsigned)fu.i - (unsigned)FLOOR_BIAS * (unsigned)BOX_W;
+                const float v0 = m.v0;
+#pragma unroll
+                for (int z = 0; z < TB_Z; ++z) {
+                    const float fz = (float)z;
+                    const float lv = fmaf(r1.z, fz, vb) * rw - v0;
+                    const FloorFrac fv = floor_frac(lv);
+                    unsigned idx = (unsigned)fv.bits * (unsigned)BOX_W + col;
+                    idx = min(idx, MAX_IDX);  // memory safety only: the margin keeps idx in range
+                    const float p00 = smem_to_float(tile + idx);
+                    const float p01 = smem_to_float(tile + idx + 1);
+                    const float p10 = smem_to_float(tile + idx + BOX_W);
+                    const float p11 = smem_to_float(tile + idx + BOX_W + 1);
+                    const float val = lerp_ref(lerp_ref(p00, p01, tx), lerp_ref(p10, p11, tx), fv.f);
+                    acc[z] = fmaf(val * rw, rw, acc[z]);
+                }
+            } else if (mode == MODE_SMEM) {
                 const T *tile = &tiles[cur][k][0];
                 const float u0 = m.u0, v0 = m.v0;
 #pragma unroll

@@ -8,12 +8,13 @@
 // sample at nearly the same (x, y) and at consecutive z whenever the
 // detector's v axis runs along z -- true for every view of a circular
 // trajectory.  Such views ("z mode") lay warps along v and read a z-fastest
-// copy that stores the tap PAIR (V(z), V(z+1)) in each element, so a sample is
-// four pair loads whose warp-wide footprint is a few sectors.
+// copy of trilinear CELLS: the element of cell (x, y, z) holds all eight taps
+// V(x + {0,1}, y + {0,1}, z + {0,1}), so a sample is ONE 16-byte load (two
+// for FP32) whose warp-wide footprint is a few consecutive lines.
 // Other views ("xy mode") lay warps along u and read an x-fastest or a
 // y-fastest copy, whichever fastest axis runs across their rays.
-// All copies carry a zero border (one voxel below, two above in x, y, z), so
-// the taps of any sample inside the box [0, N] need no bounds test; they are
+// All copies carry a zero border, so the taps of any sample inside the box
+// [0, N] need no bounds test; they are
 // written into the workspace per batch element, and a copy no view needs is
 // skipped on the device.  Sample positions, weights and the march are those
 // of cone_ray.cuh (FP64 ray set-up, FP32 alpha advanced as the reference
@@ -31,6 +32,11 @@ namespace {
 constexpr int PB_X = 32;
 constexpr int PB_Y = 8;
 constexpr int PAD_TILE = 32;
+// Views per chunk of the block order (see cone_fp_padded_kernel).
+#ifndef PYRONN_FP_VIEW_CHUNK
+#define PYRONN_FP_VIEW_CHUNK 32
+#endif
+constexpr int VIEW_CHUNK = PYRONN_FP_VIEW_CHUNK;
 
 // workspace header words (after the error flag) set by classify_views_kernel
 enum { FLAG_NEED_XY = 1, FLAG_NEED_Z = 2 };
@@ -50,76 +56,109 @@ __global__ void classify_views_kernel(const ConeFpView *__restrict__ views, int 
     atomicOr(&flags[view_is_z_mode(views[t]) ? FLAG_NEED_Z : FLAG_NEED_XY], 1u);
 }
 
-// (V(z), V(z+1)) tap pairs: a float2 for FP32, a 32-bit word of two 16-bit
-// values for BF16 / FP16 (the lower-addressed value in the low half)
-template <typename T>
-struct TapPair;
-template <>
-struct TapPair<float> {
-    using type = float2;
-    __device__ static float2 make(float a, float b) { return make_float2(a, b); }
-    __device__ static void unpack(const float2 &w, float &lo, float &hi)
-    {
-        lo = w.x;
-        hi = w.y;
-    }
-};
-template <>
-struct TapPair<__nv_bfloat16> {
-    using type = unsigned;
-    __device__ static unsigned make(__nv_bfloat16 a, __nv_bfloat16 b)
-    {
-        return (unsigned)__bfloat16_as_ushort(a) | ((unsigned)__bfloat16_as_ushort(b) << 16);
-    }
-    __device__ static void unpack(unsigned w, float &lo, float &hi)
-    {
-        lo = __uint_as_float(w << 16);
-        hi = __uint_as_float(w & 0xFFFF0000u);
-    }
-};
-template <>
-struct TapPair<__half> {
-    using type = unsigned;
-    __device__ static unsigned make(__half a, __half b)
-    {
-        return (unsigned)__half_as_ushort(a) | ((unsigned)__half_as_ushort(b) << 16);
-    }
-    __device__ static void unpack(unsigned w, float &lo, float &hi)
-    {
-        lo = __half2float(__ushort_as_half((unsigned short)(w & 0xFFFFu)));
-        hi = __half2float(__ushort_as_half((unsigned short)(w >> 16)));
-    }
+// The eight taps of a trilinear cell, as (x0, x1) pairs in the order
+// (y0 z0), (y0 z1), (y1 z0), (y1 z1): two float4 for FP32, four 32-bit words
+// of two 16-bit values for BF16 / FP16 (x0 in the low half).
+struct alignas(16) CellF32 {
+    float4 y0, y1;  // (x0 z0, x1 z0, x0 z1, x1 z1) at y0, then at y1
 };
 
-// z-fastest pair copy: element [xp][yp][zq] = (V(xp-1, yp-1, zq-1), V(xp-1, yp-1, zq)),
-// xp in [0, X+2], yp in [0, Y+2], zq in [0, Z+1], V zero outside the volume.
-// Reads run along x, writes along z: a 32 x 33 tile is transposed through
-// shared memory.  Skipped when no view is in z mode.
 template <typename T>
-__global__ void __launch_bounds__(PAD_TILE *8) pad_zpairs_kernel(const T *__restrict__ src,
-                                                                  typename TapPair<T>::type *__restrict__ dst, int X,
-                                                                  int Y, int Z, const unsigned *__restrict__ flags)
+struct Cell;
+template <>
+struct Cell<float> {
+    using type = CellF32;
+    __device__ static void load(const CellF32 *c, float (&v)[8])
+    {
+        const float4 a = __ldg(&c->y0), b = __ldg(&c->y1);
+        v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+    }
+    __device__ static CellF32 make(const float (&v)[8])
+    {
+        CellF32 c;
+        c.y0 = make_float4(v[0], v[1], v[2], v[3]);
+        c.y1 = make_float4(v[4], v[5], v[6], v[7]);
+        return c;
+    }
+};
+template <>
+struct Cell<__nv_bfloat16> {
+    using type = uint4;
+    __device__ static void load(const uint4 *c, float (&v)[8])
+    {
+        const uint4 w = __ldg(c);
+        const unsigned ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            v[2 * k] = __uint_as_float(ws[k] << 16);
+            v[2 * k + 1] = __uint_as_float(ws[k] & 0xFFFF0000u);
+        }
+    }
+    __device__ static uint4 make(const __nv_bfloat16 (&v)[8])
+    {
+        unsigned w[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            w[k] = (unsigned)__bfloat16_as_ushort(v[2 * k]) | ((unsigned)__bfloat16_as_ushort(v[2 * k + 1]) << 16);
+        return make_uint4(w[0], w[1], w[2], w[3]);
+    }
+};
+template <>
+struct Cell<__half> {
+    using type = uint4;
+    __device__ static void load(const uint4 *c, float (&v)[8])
+    {
+        const uint4 w = __ldg(c);
+        const unsigned ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            v[2 * k] = __half2float(__ushort_as_half((unsigned short)(ws[k] & 0xFFFFu)));
+            v[2 * k + 1] = __half2float(__ushort_as_half((unsigned short)(ws[k] >> 16)));
+        }
+    }
+    __device__ static uint4 make(const __half (&v)[8])
+    {
+        unsigned w[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            w[k] = (unsigned)__half_as_ushort(v[2 * k]) | ((unsigned)__half_as_ushort(v[2 * k + 1]) << 16);
+        return make_uint4(w[0], w[1], w[2], w[3]);
+    }
+};
+// z-fastest cell copy: element [xc][yc][zc], xc in [0, X+1], yc in [0, Y+1],
+// zc in [0, Z+1], holds the cell whose low corner is voxel (xc-1, yc-1, zc-1)
+// (V zero outside the volume), i.e. the taps of every floor in [-1, N].
+// A block reads a 33 (x) x 33 (z) x 2 (y) tile along x and writes 32 (z) x
+// 32 (x) cells along z.  Skipped when no view is in z mode.
+template <typename T>
+__global__ void __launch_bounds__(PAD_TILE *8) pad_cells_kernel(const T *__restrict__ src,
+                                                                 typename Cell<T>::type *__restrict__ dst, int X,
+                                                                 int Y, int Z, const unsigned *__restrict__ flags)
 {
     if (!flags[FLAG_NEED_Z]) return;
-    __shared__ T tile[PAD_TILE + 1][PAD_TILE + 1];  // [z][x]
-    const int Yp = Y + 3, Zq = Z + 2;
-    const int xp0 = blockIdx.x * PAD_TILE, yp = blockIdx.y, zq0 = blockIdx.z * PAD_TILE;
-    const int y = yp - 1;
-    const bool yin = y >= 0 && y < Y;
-    for (int r = threadIdx.y; r < PAD_TILE + 1; r += 8) {
-        const int z = zq0 - 1 + r, x = xp0 - 1 + threadIdx.x;
-        T v = T(0.0f);
-        if (yin && z >= 0 && z < Z && x >= 0 && x < X) v = src[((size_t)z * Y + y) * X + x];
-        tile[r][threadIdx.x] = v;
+    __shared__ T tile[2][PAD_TILE + 1][PAD_TILE + 2];  // [y - (yc-1)][z - (zc0-1)][x - (xc0-1)]
+    const int Yc = Y + 2, Zc = Z + 2;
+    const int xc0 = blockIdx.x * PAD_TILE, yc = blockIdx.y, zc0 = blockIdx.z * PAD_TILE;
+    for (int rr = threadIdx.y; rr < 2 * (PAD_TILE + 1); rr += 8) {
+        const int dy = rr / (PAD_TILE + 1), r = rr % (PAD_TILE + 1);
+        const int y = yc - 1 + dy, z = zc0 - 1 + r;
+        const bool yz_in = y >= 0 && y < Y && z >= 0 && z < Z;
+        for (int c = threadIdx.x; c < PAD_TILE + 1; c += PAD_TILE) {
+            const int x = xc0 - 1 + c;
+            T v = T(0.0f);
+            if (yz_in && x >= 0 && x < X) v = src[((size_t)z * Y + y) * X + x];
+            tile[dy][r][c] = v;
+        }
     }
     __syncthreads();
-    const int zq = zq0 + threadIdx.x;
-    if (zq < Zq) {
-        for (int c = threadIdx.y; c < PAD_TILE; c += 8) {
-            const int xp = xp0 + c;
-            if (xp < X + 3)
-                dst[((size_t)xp * Yp + yp) * Zq + zq] = TapPair<T>::make(tile[threadIdx.x][c], tile[threadIdx.x + 1][c]);
-        }
+    const int tz = threadIdx.x, zc = zc0 + tz;
+    if (zc >= Zc) return;
+    for (int c = threadIdx.y; c < PAD_TILE; c += 8) {
+        const int xc = xc0 + c;
+        if (xc >= X + 2) break;
+        const T v[8] = {tile[0][tz][c], tile[0][tz][c + 1], tile[0][tz + 1][c], tile[0][tz + 1][c + 1],
+                        tile[1][tz][c], tile[1][tz][c + 1], tile[1][tz + 1][c], tile[1][tz + 1][c + 1]};
+        dst[((size_t)xc * Yc + yc) * Zc + zc] = Cell<T>::make(v);
     }
 }
 
@@ -260,35 +299,37 @@ __device__ __forceinline__ bool march_inside(const ConeRay &r, int X, int Y, int
            fmaxf(y0, y1) <= Y + 0.5f && fmaxf(z0, z1) <= Z + 0.5f;
 }
 
-// Trilinear interpolation from the z-fastest pair copy: four pair loads, one
-// per (x, y) corner, each giving the two z taps.  `origin` points at the
-// element of source voxel (0, 0, 0)'s pair.
+// Trilinear interpolation from the cell copy: one cell load gives the eight
+// taps.  `origin` points at the cell of floor (0, 0, 0); the floor bias of
+// the three FloorFrac bit patterns is folded into one per-sampler offset.
 template <typename T>
-struct PairSampler {
-    const typename TapPair<T>::type *origin;
-    int s_y, s_x;  // element strides of y and x (z is fastest)
+struct CellSampler {
+    const typename Cell<T>::type *origin;
+    unsigned s_y, s_x;  // cell strides of y and x (z is fastest)
+    unsigned bias;      // -FLOOR_BIAS * (s_x + s_y + 1), modulo 2^32
+
+    __device__ CellSampler(const typename Cell<T>::type *o, int sy, int sx)
+        : origin(o), s_y((unsigned)sy), s_x((unsigned)sx),
+          bias(0u - (unsigned)FLOOR_BIAS * ((unsigned)sx + (unsigned)sy + 1u))
+    {
+    }
 
     __device__ __forceinline__ float operator()(float x, float y, float z) const
     {
         const FloorFrac fx = floor_frac(x), fy = floor_frac(y), fz = floor_frac(z);
-        const typename TapPair<T>::type *p = origin + (fx.i * s_x + fy.i * s_y + fz.i);
-        const typename TapPair<T>::type w00 = __ldg(p), w01 = __ldg(p + s_y), w10 = __ldg(p + s_x),
-                                        w11 = __ldg(p + s_x + s_y);
-        float a0, a1, b0, b1, c0, c1, d0, d1;
-        TapPair<T>::unpack(w00, a0, a1);  // (x0, y0)
-        TapPair<T>::unpack(w01, b0, b1);  // (x0, y1)
-        TapPair<T>::unpack(w10, c0, c1);  // (x1, y0)
-        TapPair<T>::unpack(w11, d0, d1);  // (x1, y1)
+        const unsigned idx = (unsigned)fx.bits * s_x + (unsigned)fy.bits * s_y + (unsigned)fz.bits + bias;
+        float v[8];
+        Cell<T>::load(origin + (int)idx, v);
         // the reference's order: lerp in z, then y, then x
-        const float z00 = lerp_ref(a0, a1, fz.f), z01 = lerp_ref(b0, b1, fz.f);
-        const float z10 = lerp_ref(c0, c1, fz.f), z11 = lerp_ref(d0, d1, fz.f);
+        const float z00 = lerp_ref(v[0], v[2], fz.f), z10 = lerp_ref(v[1], v[3], fz.f);
+        const float z01 = lerp_ref(v[4], v[6], fz.f), z11 = lerp_ref(v[5], v[7], fz.f);
         return lerp_ref(lerp_ref(z00, z01, fy.f), lerp_ref(z10, z11, fy.f), fx.f);
     }
 };
 
 template <typename T>
-struct ClampedPairSampler {
-    PairSampler<T> s;
+struct ClampedCellSampler {
+    CellSampler<T> s;
     float xmax, ymax, zmax;
     __device__ __forceinline__ float operator()(float x, float y, float z) const
     {
@@ -296,30 +337,41 @@ struct ClampedPairSampler {
     }
 };
 
-// Grid: (ceil(W/32), ceil(H/32), n_proj * 4); each 32 x 32 ray tile is four
-// blocks of 256 threads.  z mode: a warp is 32 consecutive v at one u, and the
+// Grid: one dimension, tiles_u * tiles_v * n_proj * 4 blocks; each 32 x 32
+// ray tile of a view is four blocks of 256 threads.  Block order: views in
+// chunks of VIEW_CHUNK, and inside a chunk tile by tile (u fastest) with the
+// chunk's views of a tile consecutive.  Rays of neighbouring views through
+// one detector tile cross nearly the same voxels, so blocks resident together
+// share their taps in L2 instead of each view streaming the whole volume.  z mode: a warp is 32 consecutive v at one u, and the
 // block's 8 x 32 results go through shared memory so the sinogram rows are
 // written 8 pixels at a time; xy mode: a warp is 32 consecutive u.
 template <typename T, typename Tout>
 __global__ void __launch_bounds__(PB_X *PB_Y)
     cone_fp_padded_kernel(const T *__restrict__ xfast, const T *__restrict__ yfast,
-                          const typename TapPair<T>::type *__restrict__ zpairs, Tout *__restrict__ sino,
+                          const typename Cell<T>::type *__restrict__ cells, Tout *__restrict__ sino,
                           const ConeFpView *__restrict__ views, const float *__restrict__ step_ptr,
                           const float *__restrict__ spacing_ptr, int X, int Y, int Z, int W, int H, int n_proj,
                           int geom_batch, int b)
 {
     __shared__ float out_tile[PB_Y][PB_X + 1];
-    const int p = blockIdx.z >> 2, sub = blockIdx.z & 3;
+    const int sub = blockIdx.x & 3;
+    const unsigned combo = blockIdx.x >> 2;  // (tile, view) index in the block order
+    const unsigned tiles_u = (W + 31) / 32, tiles = tiles_u * ((H + 31) / 32);
+    const unsigned chunk = combo / (VIEW_CHUNK * tiles), rem = combo - chunk * VIEW_CHUNK * tiles;
+    const unsigned chunk_views = min((unsigned)VIEW_CHUNK, (unsigned)n_proj - chunk * VIEW_CHUNK);
+    const unsigned tile = rem / chunk_views;
+    const int p = (int)(chunk * VIEW_CHUNK + (rem - tile * chunk_views));
+    const int tile_v = (int)(tile / tiles_u), tile_u = (int)(tile - (unsigned)tile_v * tiles_u);
     const int g = geom_batch == 1 ? 0 : b;
     const ConeFpView &view = views[(size_t)g * n_proj + p];
     const bool zmode = view_is_z_mode(view);
     int u, v;
     if (zmode) {
-        u = blockIdx.x * 32 + sub * PB_Y + threadIdx.y;
-        v = blockIdx.y * 32 + threadIdx.x;
+        u = tile_u * 32 + sub * PB_Y + threadIdx.y;
+        v = tile_v * 32 + threadIdx.x;
     } else {
-        u = blockIdx.x * 32 + threadIdx.x;
-        v = blockIdx.y * 32 + sub * PB_Y + threadIdx.y;
+        u = tile_u * 32 + threadIdx.x;
+        v = tile_v * 32 + sub * PB_Y + threadIdx.y;
     }
     const bool live = u < W && v < H;
     const float step = step_ptr[g];
@@ -331,9 +383,9 @@ __global__ void __launch_bounds__(PB_X *PB_Y)
         const float xmax = (float)X + 0.999f, ymax = (float)Y + 0.999f, zmax = (float)Z + 0.999f;
         const int Xp = X + 3, Yp = Y + 3;
         if (zmode) {
-            const int Zq = Z + 2;
-            const PairSampler<T> s{zpairs + (Yp + 1) * Zq + 1, Zq, Yp * Zq};
-            pixel = inside ? march_x2(ray, step, s) : march_x2(ray, step, ClampedPairSampler<T>{s, xmax, ymax, zmax});
+            const int Yc = Y + 2, Zc = Z + 2;
+            const CellSampler<T> s(cells + (Yc + 1) * Zc + 1, Zc, Yc * Zc);
+            pixel = inside ? march_x2(ray, step, s) : march_x2(ray, step, ClampedCellSampler<T>{s, xmax, ymax, zmax});
         } else {
             // rays mostly along x -> y-fastest copy
             const double cr0 = view.inv_ar[2] + 0.5 * (W - 1) * view.inv_ar[0] + 0.5 * (H - 1) * view.inv_ar[1];
@@ -359,7 +411,7 @@ __global__ void __launch_bounds__(PB_X *PB_Y)
     out_tile[threadIdx.y][threadIdx.x] = pixel;
     __syncthreads();
     const int t = threadIdx.y * PB_X + threadIdx.x;
-    const int ov = blockIdx.y * 32 + t / PB_Y, ou = blockIdx.x * 32 + sub * PB_Y + t % PB_Y;
+    const int ov = tile_v * 32 + t / PB_Y, ou = tile_u * 32 + sub * PB_Y + t % PB_Y;
     if (ov < H && ou < W) store_from_float(out + (size_t)ov * W + ou, out_tile[t % PB_Y][t / PB_Y]);
 }
 
@@ -372,25 +424,26 @@ template <typename Tin, typename Tout>
 cudaError_t launch_typed(const void *volume, void *sinogram, const Dims3D &d, const ConeFpView *views,
                          const float *step, const float *spacing, void *scratch, unsigned *flags, cudaStream_t stream)
 {
-    using Pair = typename TapPair<Tin>::type;
-    const size_t Xp = d.vol_x + 3, Yp = d.vol_y + 3, Zp = d.vol_z + 3, Zq = d.vol_z + 2;
+    using CellT = typename Cell<Tin>::type;
+    const size_t Xp = d.vol_x + 3, Yp = d.vol_y + 3, Zp = d.vol_z + 3;
+    const size_t Xc = d.vol_x + 2, Yc = d.vol_y + 2, Zc = d.vol_z + 2;
     char *base = (char *)scratch;
     Tin *xfast = (Tin *)base;
     Tin *yfast = (Tin *)(base + section_bytes(Xp * Yp * Zp * sizeof(Tin)));
-    Pair *zpairs = (Pair *)(base + 2 * section_bytes(Xp * Yp * Zp * sizeof(Tin)));
+    CellT *cells = (CellT *)(base + 2 * section_bytes(Xp * Yp * Zp * sizeof(Tin)));
     const int nviews = d.geom_batch * d.n_proj;
     classify_views_kernel<<<(nviews + 127) / 128, 128, 0, stream>>>(views, nviews, flags);
     const dim3 pblock(PAD_TILE, 8);
     const dim3 pgrid((unsigned)((Xp + PAD_TILE - 1) / PAD_TILE), (unsigned)((Yp + PAD_TILE - 1) / PAD_TILE),
                      (unsigned)Zp);
-    const dim3 zgrid((unsigned)((Xp + PAD_TILE - 1) / PAD_TILE), (unsigned)Yp, (unsigned)((Zq + PAD_TILE - 1) / PAD_TILE));
+    const dim3 cgrid((unsigned)((Xc + PAD_TILE - 1) / PAD_TILE), (unsigned)Yc, (unsigned)((Zc + PAD_TILE - 1) / PAD_TILE));
     const dim3 block(PB_X, PB_Y);
-    const dim3 grid((d.det_w + 31) / 32, (d.det_h + 31) / 32, d.n_proj * 4);
+    const unsigned grid = (unsigned)((d.det_w + 31) / 32) * (unsigned)((d.det_h + 31) / 32) * d.n_proj * 4;
     for (int b = 0; b < d.batch; ++b) {
         const Tin *src = (const Tin *)volume + (size_t)b * d.vol_z * d.vol_y * d.vol_x;
         pad_volume_kernel<Tin><<<pgrid, pblock, 0, stream>>>(src, xfast, yfast, d.vol_x, d.vol_y, d.vol_z, flags);
-        pad_zpairs_kernel<Tin><<<zgrid, pblock, 0, stream>>>(src, zpairs, d.vol_x, d.vol_y, d.vol_z, flags);
-        cone_fp_padded_kernel<Tin, Tout><<<grid, block, 0, stream>>>(xfast, yfast, zpairs, (Tout *)sinogram, views,
+        pad_cells_kernel<Tin><<<cgrid, pblock, 0, stream>>>(src, cells, d.vol_x, d.vol_y, d.vol_z, flags);
+        cone_fp_padded_kernel<Tin, Tout><<<grid, block, 0, stream>>>(xfast, yfast, cells, (Tout *)sinogram, views,
                                                                      step, spacing, d.vol_x, d.vol_y, d.vol_z,
                                                                      d.det_w, d.det_h, d.n_proj, d.geom_batch, b);
         cudaError_t e = cudaGetLastError();
@@ -404,14 +457,16 @@ cudaError_t launch_typed(const void *volume, void *sinogram, const Dims3D &d, co
 size_t cone_fp_padded_scratch_bytes(int vol_z, int vol_y, int vol_x, int in_dtype)
 {
     const size_t e = dtype_size(in_dtype);
-    const size_t plane = (size_t)(vol_x + 3) * (vol_y + 3);
-    return 2 * section_bytes(plane * (vol_z + 3) * e) + section_bytes(plane * (vol_z + 2) * 2 * e);
+    const size_t padded = (size_t)(vol_x + 3) * (vol_y + 3) * (vol_z + 3);
+    const size_t cells = (size_t)(vol_x + 2) * (vol_y + 2) * (vol_z + 2);
+    return 2 * section_bytes(padded * e) + section_bytes(cells * 8 * e);
 }
 
 bool cone_fp_padded_supported(const Dims3D &d)
 {
     const long long padded = (long long)(d.vol_x + 3) * (d.vol_y + 3) * (d.vol_z + 3);
-    return padded < (1LL << 31) - (1LL << 20) && (long long)d.n_proj * 4 <= 65535 && d.vol_z + 3 <= 65535 &&
+    const long long blocks = (long long)((d.det_w + 31) / 32) * ((d.det_h + 31) / 32) * d.n_proj * 4;
+    return padded < (1LL << 31) - (1LL << 20) && blocks < (1LL << 31) && d.vol_z + 3 <= 65535 &&
            d.vol_y + 3 <= 65535;
 }
 

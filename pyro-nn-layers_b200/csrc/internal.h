@@ -43,8 +43,9 @@ cudaError_t launch_cone_bp_prepare(const float *P, const float *spacing, const f
                                    int n_proj, ConeBpView *out, cudaStream_t stream);
 
 // 2D (proj2d.cu)
+// workspace: room for the two cell copies (pyronn_projection2d_workspace_size), or null
 cudaError_t launch_projection2d(const void *volume, void *sinogram, int in_dtype, int out_dtype, bool fan,
-                                const Dims2D &d, const Geom2D &g, cudaStream_t stream);
+                                const Dims2D &d, const Geom2D &g, void *workspace, cudaStream_t stream);
 cudaError_t launch_backprojection2d(const void *sinogram, void *volume, int in_dtype, int out_dtype, bool fan,
                                     const Dims2D &d, const Geom2D &g, cudaStream_t stream);
 

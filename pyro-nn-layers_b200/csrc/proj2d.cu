@@ -8,6 +8,16 @@
 // only when the sum is > 0, result scaled by |ray (.) spacing| (:141).
 // The reference samples a border/linear texture at index + 0.5; here the
 // same bilinear interpolation is done with exact FP32 weights.
+// Given a workspace, the call first writes two copies of the batch as
+// bilinear CELLS -- cell (x, y) holds the four taps V(x + {0,1}, y + {0,1}),
+// with zeros outside the slice -- one x-fastest and one y-fastest.  A sample
+// is then one 8-byte (16-bit storage) or 16-byte (FP32) load with no bounds
+// tests.  A warp's 32 threads are 32 neighbouring detector pixels, so at each
+// step their samples lie along the detector direction: views whose rays run
+// mostly along y read the x-fastest cells, the others the y-fastest ones, so
+// the warp's loads stay on few cache lines.  Without a workspace the taps are
+// read from the caller's slice with a bounds test each.  Taps are combined in
+// the same order on every path, so the choice does not change a result.
 //
 // Backward (ParallelBackprojection2D / FanBackprojection2D): one thread per
 // pixel, loop over views, linear interpolation along the detector row.
@@ -44,10 +54,146 @@ __device__ __forceinline__ float interp2d_border(const T *__restrict__ img, floa
     return lerp_ref(p0, p1, ty);
 }
 
+template <typename T>
+struct BorderSampler {
+    const T *img;
+    int X, Y;
+    __device__ __forceinline__ float operator()(float x, float y) const { return interp2d_border<T>(img, x, y, X, Y); }
+};
+
+// The four taps of a bilinear cell in the order V(x0,y0), V(x1,y0),
+// V(x0,y1), V(x1,y1): a float4 for FP32, two words of two 16-bit values for
+// BF16 / FP16 (x0 in the low half).
+template <typename T>
+struct Cell2;
+template <>
+struct Cell2<float> {
+    using type = float4;
+    __device__ static void load(const float4 *c, float (&v)[4])
+    {
+        const float4 w = __ldg(c);
+        v[0] = w.x, v[1] = w.y, v[2] = w.z, v[3] = w.w;
+    }
+    __device__ static float4 make(float a, float b, float c, float d) { return make_float4(a, b, c, d); }
+};
+template <>
+struct Cell2<__nv_bfloat16> {
+    using type = uint2;
+    __device__ static void load(const uint2 *c, float (&v)[4])
+    {
+        const uint2 w = __ldg(c);
+        v[0] = __uint_as_float(w.x << 16), v[1] = __uint_as_float(w.x & 0xFFFF0000u);
+        v[2] = __uint_as_float(w.y << 16), v[3] = __uint_as_float(w.y & 0xFFFF0000u);
+    }
+    __device__ static uint2 make(__nv_bfloat16 a, __nv_bfloat16 b, __nv_bfloat16 c, __nv_bfloat16 d)
+    {
+        return make_uint2((unsigned)__bfloat16_as_ushort(a) | ((unsigned)__bfloat16_as_ushort(b) << 16),
+                          (unsigned)__bfloat16_as_ushort(c) | ((unsigned)__bfloat16_as_ushort(d) << 16));
+    }
+};
+template <>
+struct Cell2<__half> {
+    using type = uint2;
+    __device__ static void load(const uint2 *c, float (&v)[4])
+    {
+        const uint2 w = __ldg(c);
+        v[0] = __half2float(__ushort_as_half((unsigned short)(w.x & 0xFFFFu)));
+        v[1] = __half2float(__ushort_as_half((unsigned short)(w.x >> 16)));
+        v[2] = __half2float(__ushort_as_half((unsigned short)(w.y & 0xFFFFu)));
+        v[3] = __half2float(__ushort_as_half((unsigned short)(w.y >> 16)));
+    }
+    __device__ static uint2 make(__half a, __half b, __half c, __half d)
+    {
+        return make_uint2((unsigned)__half_as_ushort(a) | ((unsigned)__half_as_ushort(b) << 16),
+                          (unsigned)__half_as_ushort(c) | ((unsigned)__half_as_ushort(d) << 16));
+    }
+};
+
+// Bilinear interpolation from a cell copy; `origin` is the cell of floor
+// (0, 0), (s_x, s_y) the cell strides.  Floors must lie in [-1, N].
+template <typename T>
+struct CellSampler2 {
+    const typename Cell2<T>::type *origin;
+    int s_x, s_y;
+    __device__ __forceinline__ float operator()(float x, float y) const
+    {
+        const FloorFrac fx = floor_frac(x), fy = floor_frac(y);
+        float v[4];
+        Cell2<T>::load(origin + (fx.i * s_x + fy.i * s_y), v);
+        return lerp_ref(lerp_ref(v[0], v[1], fx.f), lerp_ref(v[2], v[3], fx.f), fy.f);
+    }
+};
+
+// For rays whose march leaves [-1, N + 1): positions clamped into it, which
+// changes no tap weight that is not zero either way.
+template <typename T>
+struct ClampedCellSampler2 {
+    CellSampler2<T> s;
+    float xmax, ymax;
+    __device__ __forceinline__ float operator()(float x, float y) const
+    {
+        return s(fminf(fmaxf(x, -1.0f), xmax), fminf(fmaxf(y, -1.0f), ymax));
+    }
+};
+
+// The ray march of kernel_project2D (par_projector_2D_CudaKernel.cu.cc:58-102)
+// at positions (bx + a gx, by + a gy) in index space, two samples per
+// iteration (their gathers overlap) with the same alpha sequence and order of
+// additions as one at a time.
+template <typename F>
+__device__ __forceinline__ float march2d(float a, float am, float step, float gx, float bx, float gy, float by,
+                                         const F &sample)
+{
+    const double bound = ((double)am - (double)a) / (double)step + 4.0;
+    const int max_iter = bound > 1.0e8 ? 100000000 : (int)bound;
+    float pixel = 0.0f, px = 0.0f, py = 0.0f;
+    int iter = 0;
+    if (a < am) {
+        px = fmaf(a, gx, bx);
+        py = fmaf(a, gy, by);
+        pixel += 0.5f * sample(px, py);
+        a += step;
+        ++iter;
+    }
+    while (a < am && iter < max_iter) {
+        const float a1 = a + step;
+        if (a1 < am && iter + 1 < max_iter) {
+            const float qx = fmaf(a, gx, bx), qy = fmaf(a, gy, by);
+            px = fmaf(a1, gx, bx);
+            py = fmaf(a1, gy, by);
+            const float v0 = sample(qx, qy);
+            const float v1 = sample(px, py);
+            pixel += v0;
+            pixel += v1;
+            a = a1 + step;
+            iter += 2;
+        } else {
+            px = fmaf(a, gx, bx);
+            py = fmaf(a, gy, by);
+            pixel += sample(px, py);
+            a += step;
+            ++iter;
+        }
+    }
+    pixel *= step;
+    if (pixel > 0.0f) {  // :88-100
+        const float last_val = sample(px, py);
+        pixel -= 0.5f * step * last_val;
+        a -= step;
+        const float last_step = am - a;
+        pixel += 0.5f * last_step * last_val;
+        px = fmaf(am, gx, bx);
+        py = fmaf(am, gy, by);
+        pixel += 0.5f * last_step * sample(px, py);
+    }
+    return pixel;
+}
+
 template <typename T, typename Tout, bool FAN>
 __global__ void __launch_bounds__(FP2_BLOCK)
-    projection2d_kernel(const T *__restrict__ vol, Tout *__restrict__ sino, Geom2D geo, int X, int Y, int W,
-                        int n_proj, int geom_batch)
+    projection2d_kernel(const T *__restrict__ vol, const typename Cell2<T>::type *__restrict__ cells_x,
+                        const typename Cell2<T>::type *__restrict__ cells_y, Tout *__restrict__ sino, Geom2D geo,
+                        int X, int Y, int W, int n_proj, int geom_batch)
 {
     const int u = blockIdx.x * FP2_BLOCK + threadIdx.x;
     const int p = blockIdx.y;
@@ -101,56 +247,28 @@ __global__ void __launch_bounds__(FP2_BLOCK)
     const float dx = (float)rx, dy = (float)ry;
     float pixel = 0.0f;
     if (step > 0.0f && amin < amax) {
-        const T *img = vol + (size_t)b * X * Y;
         // sample positions in index space: idx = (src + a r - o) / s
         const float isx = 1.0f / sx, isy = 1.0f / sy;
         const float bx = (float)((srcx - ox) / sx), by = (float)((srcy - oy) / sy);
         const float gx = dx * isx, gy = dy * isy;
-        float a = (float)amin;
-        const float am = (float)amax;
-        const double bound = ((double)am - (double)a) / (double)step + 4.0;
-        const int max_iter = bound > 1.0e8 ? 100000000 : (int)bound;
-        float px = 0.0f, py = 0.0f;
-        int iter = 0;
-        if (a < am) {
-            px = fmaf(a, gx, bx);
-            py = fmaf(a, gy, by);
-            pixel += 0.5f * interp2d_border<T>(img, px, py, X, Y);
-            a += step;
-            ++iter;
-        }
-        // two samples per iteration (their gathers overlap); same alpha
-        // sequence and the same order of additions as one at a time
-        while (a < am && iter < max_iter) {
-            const float a1 = a + step;
-            if (a1 < am && iter + 1 < max_iter) {
-                const float qx = fmaf(a, gx, bx), qy = fmaf(a, gy, by);
-                px = fmaf(a1, gx, bx);
-                py = fmaf(a1, gy, by);
-                const float v0 = interp2d_border<T>(img, qx, qy, X, Y);
-                const float v1 = interp2d_border<T>(img, px, py, X, Y);
-                pixel += v0;
-                pixel += v1;
-                a = a1 + step;
-                iter += 2;
-            } else {
-                px = fmaf(a, gx, bx);
-                py = fmaf(a, gy, by);
-                pixel += interp2d_border<T>(img, px, py, X, Y);
-                a += step;
-                ++iter;
-            }
-        }
-        pixel *= step;
-        if (pixel > 0.0f) {  // :88-100
-            const float last_val = interp2d_border<T>(img, px, py, X, Y);
-            pixel -= 0.5f * step * last_val;
-            a -= step;
-            const float last_step = am - a;
-            pixel += 0.5f * last_step * last_val;
-            px = fmaf(am, gx, bx);
-            py = fmaf(am, gy, by);
-            pixel += 0.5f * last_step * interp2d_border<T>(img, px, py, X, Y);
+        const float a = (float)amin, am = (float)amax;
+        if (cells_x) {
+            // block-uniform layout choice: y-fastest cells when the view's
+            // rays run mostly along x (fan: the central ray)
+            const bool fast_y = fabsf(ray_in.x) > fabsf(ray_in.y);
+            const size_t slice = (size_t)(X + 2) * (Y + 2);
+            const CellSampler2<T> cs = fast_y ? CellSampler2<T>{cells_y + b * slice + (Y + 2) + 1,
+                                                                Y + 2, 1}
+                                              : CellSampler2<T>{cells_x + b * slice + (X + 2) + 1, 1, X + 2};
+            // every position of the march lies between its two end points
+            const float x0 = fmaf(a, gx, bx), y0 = fmaf(a, gy, by), x1 = fmaf(am, gx, bx), y1 = fmaf(am, gy, by);
+            const float xmax = (float)X + 0.5f, ymax = (float)Y + 0.5f;
+            const bool inside = fminf(x0, x1) >= -1.0f && fminf(y0, y1) >= -1.0f && fmaxf(x0, x1) <= xmax &&
+                                fmaxf(y0, y1) <= ymax;
+            pixel = inside ? march2d(a, am, step, gx, bx, gy, by, cs)
+                           : march2d(a, am, step, gx, bx, gy, by, ClampedCellSampler2<T>{cs, xmax, ymax});
+        } else {
+            pixel = march2d(a, am, step, gx, bx, gy, by, BorderSampler<T>{vol + (size_t)b * X * Y, X, Y});
         }
         pixel *= sqrtf((dx * sx) * (dx * sx) + (dy * sy) * (dy * sy));  // :141
     }
@@ -193,14 +311,17 @@ __global__ void __launch_bounds__(BP2_BLOCK_X *BP2_BLOCK_Y)
             const float rr = r.x * r.x + r.y * r.y;
             const float cd = cx * -r.y + cy * r.x;
             const float cr = cx * r.x + cy * r.y;
-            s = sdd * rr * cd / fmaf(sid, rr, cr);
+            s = sdd * rr * cd * fast_rcp(fmaf(sid, rr, cr));
             const float ex = fmaf(r.x, sid, cx), ey = fmaf(r.y, sid, cy);
-            w = 1.0f / fmaf(ex, ex, ey * ey);
+            w = fast_rcp(fmaf(ex, ex, ey * ey));
         }
         const float sidx = (s - dorg) * ids;
-        const float fu = floorf(sidx);
-        const float t = sidx - fu;
-        const int x0 = __float2int_rz(fu);
+        // detector positions of pixels inside the field stay far below 2^22;
+        // a pixel whose position is larger misses the row either way
+        const float sc = fminf(fmaxf(sidx, -4.0f), (float)W + 4.0f);
+        const FloorFrac ff = floor_frac(sc);
+        const float t = ff.f;
+        const int x0 = ff.i;
         const T *row = sino_b + (size_t)n * W;
         const float p0 = (unsigned)x0 < (unsigned)W ? load_as_float(row + x0) : 0.0f;
         const float p1 = (unsigned)(x0 + 1) < (unsigned)W ? load_as_float(row + x0 + 1) : 0.0f;
@@ -214,17 +335,69 @@ __global__ void __launch_bounds__(BP2_BLOCK_X *BP2_BLOCK_Y)
     store_from_float(vol + ((size_t)b * Y + j) * X + i, out);
 }
 
+// Both cell copies of the batch: cell (xc, yc), xc in [0, X+1], yc in
+// [0, Y+1], has its low corner at pixel (xc-1, yc-1).  A block loads a 33 x 33
+// tile along x and writes 32 x 32 cells x-fastest (along x) and y-fastest
+// (along y); grid (ceil((X+2)/32), ceil((Y+2)/32), batch), block 32 x 8.
+template <typename T>
+__global__ void __launch_bounds__(256) pad_cells2d_kernel(const T *__restrict__ in,
+                                                          typename Cell2<T>::type *__restrict__ cells_x,
+                                                          typename Cell2<T>::type *__restrict__ cells_y, int X, int Y)
+{
+    __shared__ T tile[33][34];  // [y - (yc0-1)][x - (xc0-1)]
+    const int Xc = X + 2, Yc = Y + 2;
+    const int xc0 = blockIdx.x * 32, yc0 = blockIdx.y * 32;
+    const T *img = in + (size_t)blockIdx.z * X * Y;
+    for (int r = threadIdx.y; r < 33; r += 8) {
+        const int y = yc0 - 1 + r;
+        for (int c = threadIdx.x; c < 33; c += 32) {
+            const int x = xc0 - 1 + c;
+            T v = T(0.0f);
+            if (y >= 0 && y < Y && x >= 0 && x < X) v = img[(size_t)y * X + x];
+            tile[r][c] = v;
+        }
+    }
+    __syncthreads();
+    const size_t slice = (size_t)blockIdx.z * Xc * Yc;
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        {  // x-fastest: thread x along xc
+            const int xc = xc0 + threadIdx.x, yc = yc0 + r;
+            if (xc < Xc && yc < Yc)
+                cells_x[slice + (size_t)yc * Xc + xc] = Cell2<T>::make(
+                    tile[r][threadIdx.x], tile[r][threadIdx.x + 1], tile[r + 1][threadIdx.x], tile[r + 1][threadIdx.x + 1]);
+        }
+        {  // y-fastest: thread x along yc
+            const int yc = yc0 + threadIdx.x, xc = xc0 + r;
+            if (xc < Xc && yc < Yc)
+                cells_y[slice + (size_t)xc * Yc + yc] = Cell2<T>::make(
+                    tile[threadIdx.x][r], tile[threadIdx.x][r + 1], tile[threadIdx.x + 1][r], tile[threadIdx.x + 1][r + 1]);
+        }
+    }
+}
+
 template <typename Tin, typename Tout>
 cudaError_t fp_typed(const void *volume, void *sinogram, bool fan, const Dims2D &d, const Geom2D &g,
-                     cudaStream_t stream)
+                     void *workspace, cudaStream_t stream)
 {
+    using C = typename Cell2<Tin>::type;
+    C *cells_x = nullptr, *cells_y = nullptr;
+    if (workspace) {
+        const size_t n = (size_t)d.batch * (d.vol_x + 2) * (d.vol_y + 2);
+        cells_x = (C *)workspace;
+        cells_y = (C *)((char *)workspace + (n * sizeof(C) + 255) / 256 * 256);
+        const dim3 tgrid((d.vol_x + 2 + 31) / 32, (d.vol_y + 2 + 31) / 32, d.batch);
+        pad_cells2d_kernel<Tin><<<tgrid, dim3(32, 8), 0, stream>>>((const Tin *)volume, cells_x, cells_y, d.vol_x,
+                                                                  d.vol_y);
+    }
     const dim3 grid((d.det_w + FP2_BLOCK - 1) / FP2_BLOCK, d.n_proj, d.batch);
     if (fan)
         projection2d_kernel<Tin, Tout, true><<<grid, FP2_BLOCK, 0, stream>>>(
-            (const Tin *)volume, (Tout *)sinogram, g, d.vol_x, d.vol_y, d.det_w, d.n_proj, d.geom_batch);
+            (const Tin *)volume, cells_x, cells_y, (Tout *)sinogram, g, d.vol_x, d.vol_y, d.det_w, d.n_proj,
+            d.geom_batch);
     else
         projection2d_kernel<Tin, Tout, false><<<grid, FP2_BLOCK, 0, stream>>>(
-            (const Tin *)volume, (Tout *)sinogram, g, d.vol_x, d.vol_y, d.det_w, d.n_proj, d.geom_batch);
+            (const Tin *)volume, cells_x, cells_y, (Tout *)sinogram, g, d.vol_x, d.vol_y, d.det_w, d.n_proj,
+            d.geom_batch);
     return cudaGetLastError();
 }
 
@@ -247,12 +420,12 @@ cudaError_t bp_typed(const void *sinogram, void *volume, bool fan, const Dims2D 
 }  // namespace
 
 cudaError_t launch_projection2d(const void *volume, void *sinogram, int in_dtype, int out_dtype, bool fan,
-                                const Dims2D &d, const Geom2D &g, cudaStream_t stream)
+                                const Dims2D &d, const Geom2D &g, void *workspace, cudaStream_t stream)
 {
     return dispatch_dtypes(in_dtype, out_dtype, [&](auto tin, auto tout) {
         using Tin = typename decltype(tin)::type;
         using Tout = typename decltype(tout)::type;
-        return fp_typed<Tin, Tout>(volume, sinogram, fan, d, g, stream);
+        return fp_typed<Tin, Tout>(volume, sinogram, fan, d, g, workspace, stream);
     });
 }
 

@@ -35,9 +35,12 @@ PROTOTYPES = {
     "pyronn_last_error": (ctypes.c_char_p, []),
     "pyronn_release_cached_arrays": (_I, []),
     "pyronn_workspace_error": (_I, [_P, _P, _P]),
-    "pyronn_parallel_projection2d": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _P]),
+    "pyronn_projection2d_workspace_size": (_SZ, [_I] * 4),
+    "pyronn_parallel_projection2d": (
+        _I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _P, _SZ, _P]),
     "pyronn_parallel_backprojection2d": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _P]),
-    "pyronn_fan_projection2d": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
+    "pyronn_fan_projection2d": (
+        _I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _I, _P, _SZ, _P]),
     "pyronn_fan_backprojection2d": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
     "pyronn_cone_projection3d_workspace_size": (_SZ, [_I] * 10),
     "pyronn_cone_projection3d": (
@@ -110,5 +113,6 @@ def call(name: str, *args) -> None:
 
 
 def workspace_size(name: str, *args: int) -> int:
-    """Workspace bytes of a cone entry point; args as the C query takes them."""
+    """Workspace bytes of an entry point (``pyronn_projection2d`` for both 2D
+    forward ops); args as the C query takes them."""
     return int(getattr(load(), name + "_workspace_size")(*args))

@@ -167,7 +167,8 @@ def _out_dtype(x: torch.Tensor, out_dtype) -> torch.dtype:
     return d
 
 
-def _run_2d(forward: bool, x: torch.Tensor, out_dims, geo: Geometry2D, out_dtype=None) -> torch.Tensor:
+def _run_2d(forward: bool, x: torch.Tensor, out_dims, geo: Geometry2D, out_dtype=None,
+            workspace=None) -> torch.Tensor:
     batch = x.shape[0]
     dev = x.device
     od = _out_dtype(x, out_dtype)
@@ -177,15 +178,21 @@ def _run_2d(forward: bool, x: torch.Tensor, out_dims, geo: Geometry2D, out_dtype
         out = torch.empty((batch, n_proj, det_w), dtype=od, device=dev)
         fn = "pyronn_fan_projection2d" if geo.fan else "pyronn_parallel_projection2d"
         dims = [batch, vol_y, vol_x, n_proj, det_w]
+        # the transposed slice copy read by views whose rays run along x
+        ws_bytes = _capi.workspace_size("pyronn_projection2d", batch, vol_y, vol_x, storage_code(x.dtype))
+        if workspace is None or workspace.numel() < ws_bytes:
+            workspace = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+        ws = [workspace.data_ptr(), workspace.numel()]
     else:
         n_proj, det_w = x.shape[1], x.shape[2]
         vol_y, vol_x = out_dims
         out = torch.empty((batch, vol_y, vol_x), dtype=od, device=dev)
         fn = "pyronn_fan_backprojection2d" if geo.fan else "pyronn_parallel_backprojection2d"
         dims = [batch, n_proj, det_w, vol_y, vol_x]
+        ws = []
     with torch.cuda.device(dev):
         _capi.call(fn, x.data_ptr(), out.data_ptr(), storage_code(x.dtype), storage_code(od), *dims,
-                   *geo.pointers(), geo.g, _stream(dev))
+                   *geo.pointers(), geo.g, *ws, _stream(dev))
     return out
 
 

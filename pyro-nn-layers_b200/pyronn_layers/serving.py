@@ -195,9 +195,11 @@ class Executor:
                     int(np.prod(self.out_shape)) * self._elem(self.out_dtype)) + self._ws_bytes(b)
 
     def _ws_bytes(self, batch: int) -> int:
-        if self.entry.kind == "fan":
-            return 0
         code = self.ops.storage_code(self.dtype)
+        if self.entry.kind == "fan":
+            if not self.fwd:
+                return 0
+            return self._capi.workspace_size("pyronn_projection2d", batch, *self.in_shape, code)
         name = "pyronn_cone_projection3d" if self.fwd else "pyronn_cone_backprojection3d"
         return self._capi.workspace_size(name, batch, *self.in_shape, *self.out_shape, code, 0, 1)
 
@@ -240,7 +242,8 @@ class Executor:
             n_proj, det_w = self.entry.sinogram_shape
             if self.fwd:
                 self._capi.call("pyronn_fan_projection2d", inp.data_ptr(), out.data_ptr(), code_in, code_out, batch,
-                                vol_y, vol_x, n_proj, det_w, *self.geo.pointers(), 1, stream_handle)
+                                vol_y, vol_x, n_proj, det_w, *self.geo.pointers(), 1, ws.data_ptr(), ws.numel(),
+                                stream_handle)
             else:
                 self._capi.call("pyronn_fan_backprojection2d", inp.data_ptr(), out.data_ptr(), code_in, code_out,
                                 batch, n_proj, det_w, vol_y, vol_x, *self.geo.pointers(), 1, stream_handle)

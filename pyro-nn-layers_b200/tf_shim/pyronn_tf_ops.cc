@@ -184,6 +184,12 @@ class Op2D : public OpKernel {
         Tensor *out = nullptr;
         const TensorShape os = kForward ? TensorShape({batch, n_proj, det_w}) : TensorShape({batch, vol_y, vol_x});
         OP_REQUIRES_OK(ctx, ctx->allocate_output(0, os, &out));
+        // forward: the transposed slice copy (see pyronn_projection2d_workspace_size)
+        Tensor ws;
+        const size_t ws_bytes = kForward ? pyronn_projection2d_workspace_size(batch, vol_y, vol_x, PYRONN_FLOAT32) : 0;
+        if (ws_bytes)
+            OP_REQUIRES_OK(ctx, ctx->allocate_temp(DT_UINT8, TensorShape({(int64)ws_bytes}), &ws));
+        void *ws_ptr = ws_bytes ? (void *)ws.flat<uint8>().data() : nullptr;
         const float *p_vo = vo.flat<float>().data(), *p_do = dor.flat<float>().data();
         const float *p_vs = vs.flat<float>().data(), *p_ds = ds.flat<float>().data();
         const float *p_r = rays.flat<float>().data();
@@ -192,7 +198,8 @@ class Op2D : public OpKernel {
             const float *sid = ctx->input(6).flat<float>().data(), *sdd = ctx->input(7).flat<float>().data();
             st = kForward ? pyronn_fan_projection2d(in.flat<float>().data(), out->flat<float>().data(),
                                                     PYRONN_FLOAT32, PYRONN_FLOAT32, batch, vol_y, vol_x, n_proj,
-                                                    det_w, p_vo, p_do, p_vs, p_ds, sid, sdd, p_r, g, StreamOf(ctx))
+                                                    det_w, p_vo, p_do, p_vs, p_ds, sid, sdd, p_r, g, ws_ptr, ws_bytes,
+                                                    StreamOf(ctx))
                           : pyronn_fan_backprojection2d(in.flat<float>().data(), out->flat<float>().data(),
                                                         PYRONN_FLOAT32, PYRONN_FLOAT32, batch, n_proj, det_w, vol_y,
                                                         vol_x, p_vo, p_do, p_vs, p_ds, sid, sdd, p_r, g,
@@ -200,7 +207,8 @@ class Op2D : public OpKernel {
         } else {
             st = kForward ? pyronn_parallel_projection2d(in.flat<float>().data(), out->flat<float>().data(),
                                                          PYRONN_FLOAT32, PYRONN_FLOAT32, batch, vol_y, vol_x, n_proj,
-                                                         det_w, p_vo, p_do, p_vs, p_ds, p_r, g, StreamOf(ctx))
+                                                         det_w, p_vo, p_do, p_vs, p_ds, p_r, g, ws_ptr, ws_bytes,
+                                                         StreamOf(ctx))
                           : pyronn_parallel_backprojection2d(in.flat<float>().data(), out->flat<float>().data(),
                                                              PYRONN_FLOAT32, PYRONN_FLOAT32, batch, n_proj, det_w,
                                                              vol_y, vol_x, p_vo, p_do, p_vs, p_ds, p_r, g,

@@ -49,11 +49,11 @@ def test_workspace_sizes():
     bp = lib.pyronn_cone_backprojection3d_workspace_size(2, 360, 100, 120, 64, 64, 64, 0, 0, 2)
     assert fp_hw >= 256 + 2 * 360 * 96 and fp_hw % 256 == 0
     # zero-padded copies of one volume for the software forward path: x- and
-    # y-fastest (67^3 each) and the z-fastest tap-pair copy (67 x 67 x 66 pairs)
+    # y-fastest (67^3 each) and the z-fastest cell copy (66^3 cells of 8 taps)
     def align(n):
         return (n + 255) // 256 * 256
-    assert fp - fp_hw == 2 * align(67 ** 3 * 4) + align(67 * 67 * 66 * 8)
-    assert fp16 - fp_hw == 2 * align(67 ** 3 * 2) + align(67 * 67 * 66 * 4)
+    assert fp - fp_hw == 2 * align(67 ** 3 * 4) + align(66 ** 3 * 32)
+    assert fp16 - fp_hw == 2 * align(67 ** 3 * 2) + align(66 ** 3 * 16)
     assert bp >= 256 + 2 * 360 * 48 and bp % 256 == 0
     assert lib.pyronn_cone_projection3d_workspace_size(0, 8, 8, 8, 10, 4, 4, 0, 0, 1) == 0
     assert lib.pyronn_cone_projection3d_workspace_size(1, 8, 8, 8, 10, 4, 4, 9, 0, 1) == 0
@@ -78,12 +78,31 @@ def test_2d_rejects_bad_arguments(in_dt, out_dt, batch, g, msg):
 
 def test_null_pointers_and_dims():
     lib = _capi.load()
-    st = lib.pyronn_parallel_projection2d(None, FAKE, 0, 0, 1, 4, 4, 3, 5, FAKE, FAKE, FAKE, FAKE, FAKE, 1, None)
+    st = lib.pyronn_parallel_projection2d(None, FAKE, 0, 0, 1, 4, 4, 3, 5, FAKE, FAKE, FAKE, FAKE, FAKE, 1, None, 0,
+                                          None)
     assert st == _capi.ERROR_INVALID_ARGUMENT and b"null data" in lib.pyronn_last_error()
-    st = lib.pyronn_parallel_projection2d(FAKE, FAKE, 0, 0, 1, 4, 4, 3, 5, FAKE, None, FAKE, FAKE, FAKE, 1, None)
+    st = lib.pyronn_parallel_projection2d(FAKE, FAKE, 0, 0, 1, 4, 4, 3, 5, FAKE, None, FAKE, FAKE, FAKE, 1, None, 0,
+                                          None)
     assert st == _capi.ERROR_INVALID_ARGUMENT and b"null geometry" in lib.pyronn_last_error()
-    st = lib.pyronn_parallel_projection2d(FAKE, FAKE, 0, 0, 1, 4, 0, 3, 5, FAKE, FAKE, FAKE, FAKE, FAKE, 1, None)
+    st = lib.pyronn_parallel_projection2d(FAKE, FAKE, 0, 0, 1, 4, 0, 3, 5, FAKE, FAKE, FAKE, FAKE, FAKE, 1, None, 0,
+                                          None)
     assert st == _capi.ERROR_INVALID_ARGUMENT and b"positive" in lib.pyronn_last_error()
+
+
+def test_2d_forward_workspace_size_and_checks():
+    lib = _capi.load()
+    # two cell copies of the batch (4 taps per cell, one-cell border), each
+    # rounded up to 256 bytes
+    assert _capi.workspace_size("pyronn_projection2d", 3, 5, 7, 0) == 2 * 3072
+    assert _capi.workspace_size("pyronn_projection2d", 2, 100, 100, 1) == 2 * 166656
+    assert _capi.workspace_size("pyronn_projection2d", 0, 5, 7, 0) == 0
+    assert _capi.workspace_size("pyronn_projection2d", 1, 5, 7, 9) == 0
+    st = lib.pyronn_fan_projection2d(FAKE, FAKE, 0, 0, 2, 10, 10, 3, 5, FAKE, FAKE, FAKE, FAKE, FAKE, FAKE, FAKE, 1,
+                                     FAKE, 2 * 4608 - 1, None)
+    assert st == _capi.ERROR_WORKSPACE_TOO_SMALL and b"9216" in lib.pyronn_last_error()
+    st = lib.pyronn_parallel_projection2d(FAKE, FAKE, 0, 0, 1, 4, 4, 3, 5, FAKE, FAKE, FAKE, FAKE, FAKE, 1, FAKE + 4,
+                                          1 << 20, None)
+    assert st == _capi.ERROR_INVALID_ARGUMENT and b"aligned" in lib.pyronn_last_error()
 
 
 def test_cone_rejects_small_workspace_and_huge_sizes():

@@ -103,6 +103,35 @@ def test_axis_aligned_rays(cuda):
     assert rel_l2(out.cpu().numpy(), ref) < 2e-5
 
 
+@pytest.mark.parametrize("fan", [False, True])
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_2d_forward_layout_choice_is_bit_exact(cuda, fan, dtype):
+    """Views whose rays run along x read the transposed slice copy (given a
+    workspace); the taps are combined in the same order, so a result is the
+    same bits with and without the workspace, for every view direction."""
+    if fan:
+        geo, x = _fan_setup(cuda, dtype)
+        fn = "pyronn_fan_projection2d"
+    else:
+        geo, x = _par_setup(cuda, dtype)
+        fn = "pyronn_parallel_projection2d"
+    gp = pl.ops.Geometry2D(x.shape[0], cuda, *geo.args()[:4], geo.args()[-1], geo.detector_shape[0],
+                           *(geo.args()[4:6] if fan else ()))
+    n_proj, det_w = geo.detector_shape
+    code = pl.ops.storage_code(dtype)
+    outs = []
+    for with_ws in (False, True):
+        out = torch.full((x.shape[0], n_proj, det_w), float("nan"), device=cuda)
+        ws_bytes = _capi.workspace_size("pyronn_projection2d", x.shape[0], *x.shape[1:], code)
+        ws = torch.full((ws_bytes,), 255, dtype=torch.uint8, device=cuda)
+        _capi.call(fn, x.data_ptr(), out.data_ptr(), code, 0, x.shape[0], *x.shape[1:], n_proj, det_w,
+                   *gp.pointers(), gp.g, ws.data_ptr() if with_ws else None, ws_bytes if with_ws else 0,
+                   torch.cuda.current_stream().cuda_stream)
+        outs.append(out.cpu())
+    assert torch.isfinite(outs[0]).all()
+    assert torch.equal(outs[0], outs[1])
+
+
 # ------------------------------------------------------------------ cone
 
 
@@ -269,7 +298,8 @@ def test_invalid_arguments_raise(cuda):
         pl.cone_projection3d(x.double(), geo.detector_shape, *geo.args())
     # geom_batch that is neither 1 nor batch, straight through the C ABI
     lib = _capi.load()
-    st = lib.pyronn_parallel_projection2d(x.data_ptr(), x.data_ptr(), 0, 0, 2, 4, 4, 3, 5, 1, 1, 1, 1, 1, 3, None)
+    st = lib.pyronn_parallel_projection2d(x.data_ptr(), x.data_ptr(), 0, 0, 2, 4, 4, 3, 5, 1, 1, 1, 1, 1, 3, None, 0,
+                                          None)
     assert st == _capi.ERROR_INVALID_ARGUMENT
     assert b"geom_batch" in lib.pyronn_last_error()
     st = lib.pyronn_cone_projection3d(x.data_ptr(), x.data_ptr(), 0, 0, 0, 1, 4, 4, 4, 3, 5, 5, 1, 1, 1, 1, 1, 1,
