@@ -56,6 +56,16 @@ WORKLOADS = {
                     sid_mm=750.0, sdd_mm=1200.0, step_voxels=0.5),
 }
 PHANTOM_ELLIPSOIDS = 32
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
+# the dominant kernel, from a one-pass ncu capture of
+#   python bench.py --steps 1 --warmup 3 --no-cpu-baseline
+# keyed by (workload, volume storage, sinogram storage, hardware_interp)
+NCU_DRAM_BYTES = {
+    ("cone512", "fp16", "fp16", False): 37.59e9 + 0.573e9,
+}
+# kernels of ours launched per fwd+back step (geometry preparation, view
+# classification, the two volume copies, forward; preparation, backprojection)
+LAUNCHES_PER_STEP = {False: 7, True: 6}
 L2_BYTES = 126 * 1024 * 1024
 
 
@@ -421,7 +431,8 @@ def run_ours(args, cfg):
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": "%s HBM copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"
                 % peak_kind if peak_kind == "measured" else "fallback 6.65 TB/s",
-                "traffic": args.traffic_bytes,
+                "traffic": args.traffic_bytes if args.traffic_bytes is not None else NCU_DRAM_BYTES.get(
+                    (args.workload, args.storage, sino_storage_name(args), hw)) if f_ms >= b_ms else None,
                 "algorithmic_bytes_per_launch": dom_bytes,
                 "note": "algorithmic bytes = interpolation taps x element size (+ output); frac > 1 means the "
                         "gathers are served on chip, traffic (ncu dram bytes) is the HBM side"}
@@ -440,7 +451,7 @@ def run_ours(args, cfg):
         "roofline": roofline,
         "e2e": {"value": e2e_value, "unit": "GUPS", "h2d_bytes_per_step": host_in.numel() * host_in.element_size(),
                 "d2h_bytes_per_step": host_out.numel() * host_out.element_size(), "steps": e2e_steps},
-        "gpu_launches": 4 * args.steps,
+        "gpu_launches": LAUNCHES_PER_STEP[hw] * args.steps,
         "clocks": clocks,
     }
 

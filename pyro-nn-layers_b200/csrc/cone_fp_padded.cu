@@ -287,6 +287,49 @@ __device__ __forceinline__ float march_x2(const ConeRay &ray, float step, const 
     return pixel * ray.mm_scale;
 }
 
+// march_x2 for a ray whose alpha sequence is exact (exact_sample_count
+// gave n): the same samples in the same order, counted instead of compared.
+template <typename F>
+__device__ __forceinline__ float march_counted_x2(const ConeRay &ray, int n, float step, const F &sample)
+{
+    float a = ray.a;
+    float px = fmaf(a, ray.dx, ray.ox), py = fmaf(a, ray.dy, ray.oy), pz = fmaf(a, ray.dz, ray.oz);
+    float pixel = 0.5f * sample(px, py, pz);
+    a += step;
+    int k = 1;
+    for (; k + 1 < n; k += 2) {
+        const float a1 = a + step;
+        const float qx = fmaf(a, ray.dx, ray.ox), qy = fmaf(a, ray.dy, ray.oy), qz = fmaf(a, ray.dz, ray.oz);
+        px = fmaf(a1, ray.dx, ray.ox);
+        py = fmaf(a1, ray.dy, ray.oy);
+        pz = fmaf(a1, ray.dz, ray.oz);
+        const float v0 = sample(qx, qy, qz), v1 = sample(px, py, pz);
+        pixel += v0;
+        pixel += v1;
+        a = a1 + step;
+    }
+    if (k < n) {
+        px = fmaf(a, ray.dx, ray.ox);
+        py = fmaf(a, ray.dy, ray.oy);
+        pz = fmaf(a, ray.dz, ray.oz);
+        pixel += sample(px, py, pz);
+        a += step;
+    }
+    pixel *= step;
+    if (pixel > 0.0f) {
+        const float last_val = sample(px, py, pz);
+        pixel -= 0.5f * step * last_val;
+        a -= step;
+        const float last_step = ray.am - a;
+        pixel += 0.5f * last_step * last_val;
+        px = fmaf(ray.am, ray.dx, ray.ox);
+        py = fmaf(ray.am, ray.dy, ray.oy);
+        pz = fmaf(ray.am, ray.dz, ray.oz);
+        pixel += 0.5f * last_step * sample(px, py, pz);
+    }
+    return pixel * ray.mm_scale;
+}
+
 // true when every point of the FP32 march lies in [-0.5, N + 0.5]: its end
 // points do (the segment between is convex) -- checked once per ray
 __device__ __forceinline__ bool march_inside(const ConeRay &r, int X, int Y, int Z)
@@ -385,7 +428,10 @@ __global__ void __launch_bounds__(PB_X *PB_Y)
         if (zmode) {
             const int Yc = Y + 2, Zc = Z + 2;
             const CellSampler<T> s(cells + (Yc + 1) * Zc + 1, Zc, Yc * Zc);
-            pixel = inside ? march_x2(ray, step, s) : march_x2(ray, step, ClampedCellSampler<T>{s, xmax, ymax, zmax});
+            const int n = inside ? exact_sample_count(ray, step) : -1;
+            pixel = n > 0    ? march_counted_x2(ray, n, step, s)
+                    : inside ? march_x2(ray, step, s)
+                             : march_x2(ray, step, ClampedCellSampler<T>{s, xmax, ymax, zmax});
         } else {
             // rays mostly along x -> y-fastest copy
             const double cr0 = view.inv_ar[2] + 0.5 * (W - 1) * view.inv_ar[0] + 0.5 * (H - 1) * view.inv_ar[1];

@@ -74,6 +74,30 @@ __device__ __forceinline__ ConeRay cone_ray_setup(const ConeFpView &view, int u,
     return ray;
 }
 
+// Number of samples of the march when its float alpha sequence is exact:
+// step a multiple of ulp(a0) and every alpha up to the one after the last
+// sample below the next power of two above a0, so each a += step adds
+// exactly and a_k = a0 + k * step.  Then the count is the number of k >= 0
+// with a0 + k * step < am (capped at max_iter like the checked loop),
+// computed here in FP64; -1 when the sequence may round.
+__device__ __forceinline__ int exact_sample_count(const ConeRay &ray, float step)
+{
+    const int bits = __float_as_int(ray.a);
+    const int e = (bits >> 23) & 0xff;
+    if (!ray.hit || bits <= 0 || e == 0 || e == 0xff || !(step > 0.0f)) return -1;
+    const double ulp = ldexp(1.0, e - 150);  // 2^(exponent - 23)
+    const double q = (double)step / ulp;    // exact (power-of-two divisor)
+    if (q != floor(q) || q > 16777216.0) return -1;
+    const double a0 = ray.a, st = step, am = ray.am, top = ldexp(1.0, e - 126);
+    double k = fmax(1.0, ceil((am - a0) / st));
+    // a0 + k * st is exact in FP64 (k < 2^31, 24-bit step): settle the
+    // rounding of the division
+    if (k > 1.0 && a0 + (k - 1.0) * st >= am) k -= 1.0;
+    if (a0 + k * st < am) k += 1.0;
+    if (!(a0 + (k - 1.0) * st < am) || !(a0 + k * st >= am) || a0 + k * st >= top) return -1;
+    return k > (double)ray.max_iter ? ray.max_iter : (int)k;
+}
+
 // sum of one ray; sample(x, y, z) returns the interpolated value at a point
 template <bool Linear, typename F>
 __device__ __forceinline__ float cone_ray_march(const ConeRay &ray, float step, const F &sample)

@@ -10,7 +10,11 @@
 // same bilinear interpolation is done with exact FP32 weights.
 // Given a workspace, the call first writes two copies of the batch as
 // bilinear CELLS -- cell (x, y) holds the four taps V(x + {0,1}, y + {0,1}),
-// with zeros outside the slice -- one x-fastest and one y-fastest.  A sample
+// with zeros outside the slice, for floors x, y in [-2, N] -- one x-fastest
+// and one y-fastest.  (The box starts half a millimetre below pixel 0: at
+// index -1 for 0.5 mm pixels, where rounding puts some rays' first sample a
+// hair below -1; the second border cell keeps every ray of such a view, and
+// so every lane of its warps, on the unclamped path.)  A sample
 // is then one 8-byte (16-bit storage) or 16-byte (FP32) load with no bounds
 // tests.  A warp's 32 threads are 32 neighbouring detector pixels, so at each
 // step their samples lie along the detector direction: views whose rays run
@@ -110,7 +114,7 @@ struct Cell2<__half> {
 };
 
 // Bilinear interpolation from a cell copy; `origin` is the cell of floor
-// (0, 0), (s_x, s_y) the cell strides.  Floors must lie in [-1, N].
+// (0, 0), (s_x, s_y) the cell strides.  Floors must lie in [-2, N].
 template <typename T>
 struct CellSampler2 {
     const typename Cell2<T>::type *origin;
@@ -124,15 +128,15 @@ struct CellSampler2 {
     }
 };
 
-// For rays whose march leaves [-1, N + 1): positions clamped into it, which
-// changes no tap weight that is not zero either way.
+// For rays whose march leaves [-1.5, N + 0.5]: positions clamped into it,
+// which changes no tap weight that is not zero either way.
 template <typename T>
 struct ClampedCellSampler2 {
     CellSampler2<T> s;
     float xmax, ymax;
     __device__ __forceinline__ float operator()(float x, float y) const
     {
-        return s(fminf(fmaxf(x, -1.0f), xmax), fminf(fmaxf(y, -1.0f), ymax));
+        return s(fminf(fmaxf(x, -1.5f), xmax), fminf(fmaxf(y, -1.5f), ymax));
     }
 };
 
@@ -256,14 +260,13 @@ __global__ void __launch_bounds__(FP2_BLOCK)
             // block-uniform layout choice: y-fastest cells when the view's
             // rays run mostly along x (fan: the central ray)
             const bool fast_y = fabsf(ray_in.x) > fabsf(ray_in.y);
-            const size_t slice = (size_t)(X + 2) * (Y + 2);
-            const CellSampler2<T> cs = fast_y ? CellSampler2<T>{cells_y + b * slice + (Y + 2) + 1,
-                                                                Y + 2, 1}
-                                              : CellSampler2<T>{cells_x + b * slice + (X + 2) + 1, 1, X + 2};
+            const size_t slice = (size_t)(X + 3) * (Y + 3);
+            const CellSampler2<T> cs = fast_y ? CellSampler2<T>{cells_y + b * slice + 2 * (Y + 3) + 2, Y + 3, 1}
+                                              : CellSampler2<T>{cells_x + b * slice + 2 * (X + 3) + 2, 1, X + 3};
             // every position of the march lies between its two end points
             const float x0 = fmaf(a, gx, bx), y0 = fmaf(a, gy, by), x1 = fmaf(am, gx, bx), y1 = fmaf(am, gy, by);
             const float xmax = (float)X + 0.5f, ymax = (float)Y + 0.5f;
-            const bool inside = fminf(x0, x1) >= -1.0f && fminf(y0, y1) >= -1.0f && fmaxf(x0, x1) <= xmax &&
+            const bool inside = fminf(x0, x1) >= -1.5f && fminf(y0, y1) >= -1.5f && fmaxf(x0, x1) <= xmax &&
                                 fmaxf(y0, y1) <= ymax;
             pixel = inside ? march2d(a, am, step, gx, bx, gy, by, cs)
                            : march2d(a, am, step, gx, bx, gy, by, ClampedCellSampler2<T>{cs, xmax, ymax});
@@ -335,23 +338,23 @@ __global__ void __launch_bounds__(BP2_BLOCK_X *BP2_BLOCK_Y)
     store_from_float(vol + ((size_t)b * Y + j) * X + i, out);
 }
 
-// Both cell copies of the batch: cell (xc, yc), xc in [0, X+1], yc in
-// [0, Y+1], has its low corner at pixel (xc-1, yc-1).  A block loads a 33 x 33
+// Both cell copies of the batch: cell (xc, yc), xc in [0, X+2], yc in
+// [0, Y+2], has its low corner at pixel (xc-2, yc-2).  A block loads a 33 x 33
 // tile along x and writes 32 x 32 cells x-fastest (along x) and y-fastest
-// (along y); grid (ceil((X+2)/32), ceil((Y+2)/32), batch), block 32 x 8.
+// (along y); grid (ceil((X+3)/32), ceil((Y+3)/32), batch), block 32 x 8.
 template <typename T>
 __global__ void __launch_bounds__(256) pad_cells2d_kernel(const T *__restrict__ in,
                                                           typename Cell2<T>::type *__restrict__ cells_x,
                                                           typename Cell2<T>::type *__restrict__ cells_y, int X, int Y)
 {
-    __shared__ T tile[33][34];  // [y - (yc0-1)][x - (xc0-1)]
-    const int Xc = X + 2, Yc = Y + 2;
+    __shared__ T tile[33][34];  // [y - (yc0-2)][x - (xc0-2)]
+    const int Xc = X + 3, Yc = Y + 3;
     const int xc0 = blockIdx.x * 32, yc0 = blockIdx.y * 32;
     const T *img = in + (size_t)blockIdx.z * X * Y;
     for (int r = threadIdx.y; r < 33; r += 8) {
-        const int y = yc0 - 1 + r;
+        const int y = yc0 - 2 + r;
         for (int c = threadIdx.x; c < 33; c += 32) {
-            const int x = xc0 - 1 + c;
+            const int x = xc0 - 2 + c;
             T v = T(0.0f);
             if (y >= 0 && y < Y && x >= 0 && x < X) v = img[(size_t)y * X + x];
             tile[r][c] = v;
@@ -382,10 +385,10 @@ cudaError_t fp_typed(const void *volume, void *sinogram, bool fan, const Dims2D 
     using C = typename Cell2<Tin>::type;
     C *cells_x = nullptr, *cells_y = nullptr;
     if (workspace) {
-        const size_t n = (size_t)d.batch * (d.vol_x + 2) * (d.vol_y + 2);
+        const size_t n = (size_t)d.batch * (d.vol_x + 3) * (d.vol_y + 3);
         cells_x = (C *)workspace;
         cells_y = (C *)((char *)workspace + (n * sizeof(C) + 255) / 256 * 256);
-        const dim3 tgrid((d.vol_x + 2 + 31) / 32, (d.vol_y + 2 + 31) / 32, d.batch);
+        const dim3 tgrid((d.vol_x + 3 + 31) / 32, (d.vol_y + 3 + 31) / 32, d.batch);
         pad_cells2d_kernel<Tin><<<tgrid, dim3(32, 8), 0, stream>>>((const Tin *)volume, cells_x, cells_y, d.vol_x,
                                                                   d.vol_y);
     }

@@ -153,6 +153,21 @@ def test_cone_projection_vs_oracle(cuda, dtype, hw):
     assert rel_l2(out.cpu().numpy(), ref) < tol
 
 
+@pytest.mark.parametrize("sid,step", [(160.0, 0.5), (160.0, 0.37), (128.0, 0.5)])
+def test_cone_projection_alpha_sequences(cuda, sid, step):
+    """The forward counts a ray's samples when its float alpha sequence is
+    exact (step a multiple of ulp(alpha), alphas inside one binade: SID 160
+    with step 0.5) and compares alpha against the exit otherwise (step 0.37;
+    SID 128, where the march crosses alpha = 128): both match the oracle's
+    float alpha march."""
+    geo = geometry.ConeBeam3D((20, 24, 28), (1.0, 0.9, 1.1), (30, 36), (1.2, 1.3), 16, sid, sid + 100.0,
+                              step_size=step)
+    vol = phantoms.ellipsoid_phantom_3d(geo.volume_shape, geo.volume_spacing, seed=3, n=6)[0][None]
+    out = pl.cone_projection3d(t(vol, cuda), geo.detector_shape, *geo.args())
+    ref = oracle.cone_projection3d(vol, geo.detector_shape, *geo.args())
+    assert rel_l2(out.cpu().numpy(), ref) < 2e-5
+
+
 @pytest.mark.parametrize("hw", [False, True])
 @pytest.mark.parametrize("dtype", DTYPES)
 def test_cone_backprojection_vs_oracle(cuda, dtype, hw):
