@@ -2,8 +2,8 @@
 // tiles (software interpolation, the reference's default hardware_interp=false
 // path, cone_backprojector_3D_CudaKernel.cu.cc:84-118).
 //
-// Block = 256 threads = 32 (x) x 8 (y) voxels, each thread walks 8 voxels
-// along z: a 32 x 8 x 8 voxel tile.  Views are processed in passes of
+// Block = 256 threads = 32 (x) x 8 (y) voxels, each thread walks 16 voxels
+// along z: a 32 x 8 x 16 voxel tile.  Views are processed in passes of
 // BP_K views.  For every view of a pass one warp projects the 8 tile corners,
 // takes the bounding box of the taps the tile can touch (+1 pixel margin), and
 // one thread issues a 3D TMA load of a BW x BH detector box around it into
@@ -21,7 +21,7 @@
 //
 // Views whose u and w rows have a zero z coefficient -- every view of a
 // circular trajectory about the z axis -- take a column loop: 1/w, u, the u
-// tap and its weight are then the same for the thread's 8 voxels and are
+// tap and its weight are then the same for the thread's 16 voxels and are
 // computed once; the values are exactly those of the general loop, so is the
 // result.
 #include <cuda.h>
@@ -36,7 +36,7 @@ namespace {
 
 constexpr int TB_X = 32;
 constexpr int TB_Y = 8;
-constexpr int TB_Z = 8;  // voxels per thread along z
+constexpr int TB_Z = 16;  // voxels per thread along z
 constexpr int BP_K = 4;  // views per pass
 constexpr int BOX_W = 72;  // 72-element rows shift banks between rows (64 would alias them)
 constexpr int BOX_H = 24;

@@ -12,7 +12,12 @@
 // read as zero, lerps in the reference's FMA form.  Hardware interpolation
 // (hardware_interp = true) samples a 3D texture at p + 0.5 with border
 // addressing and box [-0.5, N-0.5], as
-// cone_projector_3D_CudaKernel_hardware_interp.cu.cc:43-142 does.
+// cone_projector_3D_CudaKernel_hardware_interp.cu.cc:43-142 does; its kernel
+// runs the block order of the cell forward projector (cone_ray.cuh:
+// neighbouring views of a detector tile together) with warps along detector
+// u -- the texture's block-linear layout keeps x/y neighbours close, z
+// neighbours far, so warps along v are 1.7x slower here -- and the counted
+// march where the alpha sequence is exact.
 #include <math_constants.h>
 
 #include "common.cuh"
@@ -87,12 +92,49 @@ __global__ void __launch_bounds__(FP_BLOCK_X *FP_BLOCK_Y)
     store_from_float(sino + (((size_t)b * n_proj + p) * H + v) * (size_t)W + u, pixel);
 }
 
+static_assert(FP_BLOCK_X == 32 && FP_BLOCK_Y == 8, "the ray kernels index threads as 32 x 8");
+
+struct TexSampler {
+    cudaTextureObject_t tex;
+    __device__ __forceinline__ float operator()(float x, float y, float z) const
+    {
+        return tex3D<float>(tex, x + 0.5f, y + 0.5f, z + 0.5f);
+    }
+};
+
+// hardware_interp forward of batch element b: grid ray_block_count blocks of
+// 32 x 8 threads, a warp is 32 consecutive u
+template <typename Tout>
+__global__ void __launch_bounds__(256)
+    cone_fp_tex_kernel(cudaTextureObject_t tex, Tout *__restrict__ sino, const ConeFpView *__restrict__ views,
+                       const float *__restrict__ step_ptr, const float *__restrict__ spacing_ptr, int X, int Y,
+                       int Z, int W, int H, int n_proj, int geom_batch, int b)
+{
+    const RayBlock rb = ray_block(blockIdx.x, W, H, n_proj);
+    const int u = rb.tile_u * 32 + threadIdx.x, v = rb.tile_v * 32 + rb.sub * 8 + threadIdx.y;
+    if (u >= W || v >= H) return;
+    const int g = geom_batch == 1 ? 0 : b;
+    const float step = step_ptr[g];
+    const ConeRay ray = cone_ray_setup(views[(size_t)g * n_proj + rb.p], u, v, X, Y, Z, -0.5, step,
+                                       spacing_ptr[g * 3 + 2], spacing_ptr[g * 3 + 1], spacing_ptr[g * 3 + 0]);
+    const TexSampler s{tex};
+    const int n = exact_sample_count(ray, step);
+    const float pixel = n > 0 ? march_counted_x2(ray, n, step, s) : march_x2(ray, step, s);
+    store_from_float(sino + (((size_t)b * n_proj + rb.p) * H + v) * (size_t)W + u, pixel);
+}
+
 template <typename Tin, typename Tout>
 cudaError_t launch_typed(const void *volume, void *sinogram, const Dims3D &d, int batch_begin, int batch_count,
                          const ConeFpView *views, const float *step, const float *spacing, cudaTextureObject_t tex,
                          cudaStream_t stream)
 {
-    const dim3 block(FP_BLOCK_X, FP_BLOCK_Y, 1);
+    const dim3 block(FP_BLOCK_X, FP_BLOCK_Y, 1);  // 32 x 8, the layout both kernels index by
+    if (tex && ray_blocks_fit(d.det_w, d.det_h, d.n_proj)) {  // the texture holds batch element batch_begin
+        cone_fp_tex_kernel<Tout><<<ray_block_count(d.det_w, d.det_h, d.n_proj), block, 0, stream>>>(
+            tex, (Tout *)sinogram, views, step, spacing, d.vol_x, d.vol_y, d.vol_z, d.det_w, d.det_h, d.n_proj,
+            d.geom_batch, batch_begin);
+        return cudaGetLastError();
+    }
     // grid.z covers (batch, view) pairs, at most 65535 per launch
     const int per_launch = (65535 / d.n_proj) > 0 ? (65535 / d.n_proj) : 1;
     for (int b0 = 0; b0 < batch_count; b0 += per_launch) {

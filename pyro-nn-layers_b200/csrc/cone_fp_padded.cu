@@ -32,22 +32,8 @@ namespace {
 constexpr int PB_X = 32;
 constexpr int PB_Y = 8;
 constexpr int PAD_TILE = 32;
-// Views per chunk of the block order (see cone_fp_padded_kernel).
-#ifndef PYRONN_FP_VIEW_CHUNK
-#define PYRONN_FP_VIEW_CHUNK 32
-#endif
-constexpr int VIEW_CHUNK = PYRONN_FP_VIEW_CHUNK;
-
 // workspace header words (after the error flag) set by classify_views_kernel
 enum { FLAG_NEED_XY = 1, FLAG_NEED_Z = 2 };
-
-// Z-mode test of a view: the ray direction's derivative along detector v,
-// inv_ar (0, 1, 0) in voxel-index space, points along z.
-__device__ __forceinline__ bool view_is_z_mode(const ConeFpView &v)
-{
-    const double cx = v.inv_ar[1], cy = v.inv_ar[4], cz = v.inv_ar[7];
-    return cz * cz >= 0.81 * (cx * cx + cy * cy + cz * cz);
-}
 
 __global__ void classify_views_kernel(const ConeFpView *__restrict__ views, int n, unsigned *__restrict__ flags)
 {
@@ -239,97 +225,6 @@ struct ClampedSampler {
     }
 };
 
-// The reference's march (cone_ray.cuh) with the main loop taking two
-// samples per iteration, so the gathers of both are in flight together; the
-// alpha sequence and the order of the additions are unchanged.
-template <typename F>
-__device__ __forceinline__ float march_x2(const ConeRay &ray, float step, const F &sample)
-{
-    if (!ray.hit) return 0.0f;
-    float a = ray.a;
-    float px = fmaf(a, ray.dx, ray.ox), py = fmaf(a, ray.dy, ray.oy), pz = fmaf(a, ray.dz, ray.oz);
-    float pixel = 0.5f * sample(px, py, pz);
-    a += step;
-    int iter = 1;
-    while (a < ray.am && iter < ray.max_iter) {
-        const float a1 = a + step;
-        if (a1 < ray.am && iter + 1 < ray.max_iter) {
-            const float qx = fmaf(a, ray.dx, ray.ox), qy = fmaf(a, ray.dy, ray.oy), qz = fmaf(a, ray.dz, ray.oz);
-            px = fmaf(a1, ray.dx, ray.ox);
-            py = fmaf(a1, ray.dy, ray.oy);
-            pz = fmaf(a1, ray.dz, ray.oz);
-            const float v0 = sample(qx, qy, qz), v1 = sample(px, py, pz);
-            pixel += v0;
-            pixel += v1;
-            a = a1 + step;
-            iter += 2;
-        } else {
-            px = fmaf(a, ray.dx, ray.ox);
-            py = fmaf(a, ray.dy, ray.oy);
-            pz = fmaf(a, ray.dz, ray.oz);
-            pixel += sample(px, py, pz);
-            a += step;
-            ++iter;
-        }
-    }
-    pixel *= step;
-    if (pixel > 0.0f) {
-        const float last_val = sample(px, py, pz);
-        pixel -= 0.5f * step * last_val;
-        a -= step;
-        const float last_step = ray.am - a;
-        pixel += 0.5f * last_step * last_val;
-        px = fmaf(ray.am, ray.dx, ray.ox);
-        py = fmaf(ray.am, ray.dy, ray.oy);
-        pz = fmaf(ray.am, ray.dz, ray.oz);
-        pixel += 0.5f * last_step * sample(px, py, pz);
-    }
-    return pixel * ray.mm_scale;
-}
-
-// march_x2 for a ray whose alpha sequence is exact (exact_sample_count
-// gave n): the same samples in the same order, counted instead of compared.
-template <typename F>
-__device__ __forceinline__ float march_counted_x2(const ConeRay &ray, int n, float step, const F &sample)
-{
-    float a = ray.a;
-    float px = fmaf(a, ray.dx, ray.ox), py = fmaf(a, ray.dy, ray.oy), pz = fmaf(a, ray.dz, ray.oz);
-    float pixel = 0.5f * sample(px, py, pz);
-    a += step;
-    int k = 1;
-    for (; k + 1 < n; k += 2) {
-        const float a1 = a + step;
-        const float qx = fmaf(a, ray.dx, ray.ox), qy = fmaf(a, ray.dy, ray.oy), qz = fmaf(a, ray.dz, ray.oz);
-        px = fmaf(a1, ray.dx, ray.ox);
-        py = fmaf(a1, ray.dy, ray.oy);
-        pz = fmaf(a1, ray.dz, ray.oz);
-        const float v0 = sample(qx, qy, qz), v1 = sample(px, py, pz);
-        pixel += v0;
-        pixel += v1;
-        a = a1 + step;
-    }
-    if (k < n) {
-        px = fmaf(a, ray.dx, ray.ox);
-        py = fmaf(a, ray.dy, ray.oy);
-        pz = fmaf(a, ray.dz, ray.oz);
-        pixel += sample(px, py, pz);
-        a += step;
-    }
-    pixel *= step;
-    if (pixel > 0.0f) {
-        const float last_val = sample(px, py, pz);
-        pixel -= 0.5f * step * last_val;
-        a -= step;
-        const float last_step = ray.am - a;
-        pixel += 0.5f * last_step * last_val;
-        px = fmaf(ray.am, ray.dx, ray.ox);
-        py = fmaf(ray.am, ray.dy, ray.oy);
-        pz = fmaf(ray.am, ray.dz, ray.oz);
-        pixel += 0.5f * last_step * sample(px, py, pz);
-    }
-    return pixel * ray.mm_scale;
-}
-
 // true when every point of the FP32 march lies in [-0.5, N + 0.5]: its end
 // points do (the segment between is convex) -- checked once per ray
 __device__ __forceinline__ bool march_inside(const ConeRay &r, int X, int Y, int Z)
@@ -380,12 +275,9 @@ struct ClampedCellSampler {
     }
 };
 
-// Grid: one dimension, tiles_u * tiles_v * n_proj * 4 blocks; each 32 x 32
-// ray tile of a view is four blocks of 256 threads.  Block order: views in
-// chunks of VIEW_CHUNK, and inside a chunk tile by tile (u fastest) with the
-// chunk's views of a tile consecutive.  Rays of neighbouring views through
-// one detector tile cross nearly the same voxels, so blocks resident together
-// share their taps in L2 instead of each view streaming the whole volume.  z mode: a warp is 32 consecutive v at one u, and the
+// Grid: one dimension, ray_block_count blocks in ray_block order (four
+// blocks of 256 threads per 32 x 32 ray tile, neighbouring views of a tile
+// consecutive, cone_ray.cuh).  z mode: a warp is 32 consecutive v at one u, and the
 // block's 8 x 32 results go through shared memory so the sinogram rows are
 // written 8 pixels at a time; xy mode: a warp is 32 consecutive u.
 template <typename T, typename Tout>
@@ -397,14 +289,8 @@ __global__ void __launch_bounds__(PB_X *PB_Y)
                           int geom_batch, int b)
 {
     __shared__ float out_tile[PB_Y][PB_X + 1];
-    const int sub = blockIdx.x & 3;
-    const unsigned combo = blockIdx.x >> 2;  // (tile, view) index in the block order
-    const unsigned tiles_u = (W + 31) / 32, tiles = tiles_u * ((H + 31) / 32);
-    const unsigned chunk = combo / (VIEW_CHUNK * tiles), rem = combo - chunk * VIEW_CHUNK * tiles;
-    const unsigned chunk_views = min((unsigned)VIEW_CHUNK, (unsigned)n_proj - chunk * VIEW_CHUNK);
-    const unsigned tile = rem / chunk_views;
-    const int p = (int)(chunk * VIEW_CHUNK + (rem - tile * chunk_views));
-    const int tile_v = (int)(tile / tiles_u), tile_u = (int)(tile - (unsigned)tile_v * tiles_u);
+    const RayBlock rb = ray_block(blockIdx.x, W, H, n_proj);
+    const int p = rb.p, sub = rb.sub, tile_u = rb.tile_u, tile_v = rb.tile_v;
     const int g = geom_batch == 1 ? 0 : b;
     const ConeFpView &view = views[(size_t)g * n_proj + p];
     const bool zmode = view_is_z_mode(view);
@@ -484,7 +370,7 @@ cudaError_t launch_typed(const void *volume, void *sinogram, const Dims3D &d, co
                      (unsigned)Zp);
     const dim3 cgrid((unsigned)((Xc + PAD_TILE - 1) / PAD_TILE), (unsigned)Yc, (unsigned)((Zc + PAD_TILE - 1) / PAD_TILE));
     const dim3 block(PB_X, PB_Y);
-    const unsigned grid = (unsigned)((d.det_w + 31) / 32) * (unsigned)((d.det_h + 31) / 32) * d.n_proj * 4;
+    const unsigned grid = ray_block_count(d.det_w, d.det_h, d.n_proj);
     for (int b = 0; b < d.batch; ++b) {
         const Tin *src = (const Tin *)volume + (size_t)b * d.vol_z * d.vol_y * d.vol_x;
         pad_volume_kernel<Tin><<<pgrid, pblock, 0, stream>>>(src, xfast, yfast, d.vol_x, d.vol_y, d.vol_z, flags);
@@ -511,9 +397,8 @@ size_t cone_fp_padded_scratch_bytes(int vol_z, int vol_y, int vol_x, int in_dtyp
 bool cone_fp_padded_supported(const Dims3D &d)
 {
     const long long padded = (long long)(d.vol_x + 3) * (d.vol_y + 3) * (d.vol_z + 3);
-    const long long blocks = (long long)((d.det_w + 31) / 32) * ((d.det_h + 31) / 32) * d.n_proj * 4;
-    return padded < (1LL << 31) - (1LL << 20) && blocks < (1LL << 31) && d.vol_z + 3 <= 65535 &&
-           d.vol_y + 3 <= 65535;
+    return padded < (1LL << 31) - (1LL << 20) && ray_blocks_fit(d.det_w, d.det_h, d.n_proj) &&
+           d.vol_z + 3 <= 65535 && d.vol_y + 3 <= 65535;
 }
 
 cudaError_t launch_cone_fp_padded(const void *volume, void *sinogram, int in_dtype, int out_dtype, const Dims3D &d,

@@ -74,6 +74,148 @@ __device__ __forceinline__ ConeRay cone_ray_setup(const ConeFpView &view, int u,
     return ray;
 }
 
+// Block order of the ray-driven forward kernels.  The grid is one
+// dimension; each 32 x 32 tile of detector rays of a view is four blocks of
+// 256 threads (sub = 0..3).  Views go in chunks of VIEW_CHUNK; inside a chunk
+// the tiles follow one another (u fastest), each with the chunk's views
+// consecutive.  Rays of neighbouring views through one detector tile cross
+// nearly the same voxels, so blocks resident together share their taps in L2
+// instead of every view streaming the whole volume from DRAM.
+#ifndef PYRONN_FP_VIEW_CHUNK
+#define PYRONN_FP_VIEW_CHUNK 32
+#endif
+constexpr int VIEW_CHUNK = PYRONN_FP_VIEW_CHUNK;
+
+struct RayBlock {
+    int p;               // view
+    int tile_u, tile_v;  // 32 x 32 ray tile
+    int sub;             // quarter of the tile
+};
+
+__device__ __forceinline__ RayBlock ray_block(unsigned block, int W, int H, int n_proj)
+{
+    RayBlock rb;
+    rb.sub = (int)(block & 3u);
+    const unsigned combo = block >> 2;  // (tile, view) index in the block order
+    const unsigned tiles_u = (W + 31) / 32, tiles = tiles_u * ((H + 31) / 32);
+    const unsigned chunk = combo / (VIEW_CHUNK * tiles), rem = combo - chunk * VIEW_CHUNK * tiles;
+    const unsigned chunk_views = min((unsigned)VIEW_CHUNK, (unsigned)n_proj - chunk * VIEW_CHUNK);
+    const unsigned tile = rem / chunk_views;
+    rb.p = (int)(chunk * VIEW_CHUNK + (rem - tile * chunk_views));
+    rb.tile_v = (int)(tile / tiles_u);
+    rb.tile_u = (int)(tile - (unsigned)rb.tile_v * tiles_u);
+    return rb;
+}
+
+inline unsigned ray_block_count(int W, int H, int n_proj)
+{
+    return (unsigned)((W + 31) / 32) * (unsigned)((H + 31) / 32) * (unsigned)n_proj * 4u;
+}
+
+inline bool ray_blocks_fit(int W, int H, int n_proj)
+{
+    return (long long)((W + 31) / 32) * ((H + 31) / 32) * n_proj * 4 < (1LL << 31);
+}
+
+// Z-mode test of a view: the ray direction's derivative along detector v,
+// inv_ar (0, 1, 0) in voxel-index space, points along z.
+__device__ __forceinline__ bool view_is_z_mode(const ConeFpView &v)
+{
+    const double cx = v.inv_ar[1], cy = v.inv_ar[4], cz = v.inv_ar[7];
+    return cz * cz >= 0.81 * (cx * cx + cy * cy + cz * cz);
+}
+
+// The march of cone_ray_march<false> with the main loop taking two
+// samples per iteration, so the gathers of both are in flight together; the
+// alpha sequence and the order of the additions are unchanged.
+template <typename F>
+__device__ __forceinline__ float march_x2(const ConeRay &ray, float step, const F &sample)
+{
+    if (!ray.hit) return 0.0f;
+    float a = ray.a;
+    float px = fmaf(a, ray.dx, ray.ox), py = fmaf(a, ray.dy, ray.oy), pz = fmaf(a, ray.dz, ray.oz);
+    float pixel = 0.5f * sample(px, py, pz);
+    a += step;
+    int iter = 1;
+    while (a < ray.am && iter < ray.max_iter) {
+        const float a1 = a + step;
+        if (a1 < ray.am && iter + 1 < ray.max_iter) {
+            const float qx = fmaf(a, ray.dx, ray.ox), qy = fmaf(a, ray.dy, ray.oy), qz = fmaf(a, ray.dz, ray.oz);
+            px = fmaf(a1, ray.dx, ray.ox);
+            py = fmaf(a1, ray.dy, ray.oy);
+            pz = fmaf(a1, ray.dz, ray.oz);
+            const float v0 = sample(qx, qy, qz), v1 = sample(px, py, pz);
+            pixel += v0;
+            pixel += v1;
+            a = a1 + step;
+            iter += 2;
+        } else {
+            px = fmaf(a, ray.dx, ray.ox);
+            py = fmaf(a, ray.dy, ray.oy);
+            pz = fmaf(a, ray.dz, ray.oz);
+            pixel += sample(px, py, pz);
+            a += step;
+            ++iter;
+        }
+    }
+    pixel *= step;
+    if (pixel > 0.0f) {
+        const float last_val = sample(px, py, pz);
+        pixel -= 0.5f * step * last_val;
+        a -= step;
+        const float last_step = ray.am - a;
+        pixel += 0.5f * last_step * last_val;
+        px = fmaf(ray.am, ray.dx, ray.ox);
+        py = fmaf(ray.am, ray.dy, ray.oy);
+        pz = fmaf(ray.am, ray.dz, ray.oz);
+        pixel += 0.5f * last_step * sample(px, py, pz);
+    }
+    return pixel * ray.mm_scale;
+}
+
+// march_x2 for a ray whose alpha sequence is exact (exact_sample_count
+// gave n): the same samples in the same order, counted instead of compared.
+template <typename F>
+__device__ __forceinline__ float march_counted_x2(const ConeRay &ray, int n, float step, const F &sample)
+{
+    float a = ray.a;
+    float px = fmaf(a, ray.dx, ray.ox), py = fmaf(a, ray.dy, ray.oy), pz = fmaf(a, ray.dz, ray.oz);
+    float pixel = 0.5f * sample(px, py, pz);
+    a += step;
+    int k = 1;
+    for (; k + 1 < n; k += 2) {
+        const float a1 = a + step;
+        const float qx = fmaf(a, ray.dx, ray.ox), qy = fmaf(a, ray.dy, ray.oy), qz = fmaf(a, ray.dz, ray.oz);
+        px = fmaf(a1, ray.dx, ray.ox);
+        py = fmaf(a1, ray.dy, ray.oy);
+        pz = fmaf(a1, ray.dz, ray.oz);
+        const float v0 = sample(qx, qy, qz), v1 = sample(px, py, pz);
+        pixel += v0;
+        pixel += v1;
+        a = a1 + step;
+    }
+    if (k < n) {
+        px = fmaf(a, ray.dx, ray.ox);
+        py = fmaf(a, ray.dy, ray.oy);
+        pz = fmaf(a, ray.dz, ray.oz);
+        pixel += sample(px, py, pz);
+        a += step;
+    }
+    pixel *= step;
+    if (pixel > 0.0f) {
+        const float last_val = sample(px, py, pz);
+        pixel -= 0.5f * step * last_val;
+        a -= step;
+        const float last_step = ray.am - a;
+        pixel += 0.5f * last_step * last_val;
+        px = fmaf(ray.am, ray.dx, ray.ox);
+        py = fmaf(ray.am, ray.dy, ray.oy);
+        pz = fmaf(ray.am, ray.dz, ray.oz);
+        pixel += 0.5f * last_step * sample(px, py, pz);
+    }
+    return pixel * ray.mm_scale;
+}
+
 // Number of samples of the march when its float alpha sequence is exact:
 // step a multiple of ulp(a0) and every alpha up to the one after the last
 // sample below the next power of two above a0, so each a += step adds
