@@ -156,8 +156,10 @@ PYRONN_API int pyronn_fan_backprojection2d(const void *sinogram, void *volume, i
  *   in the reference)
  * ------------------------------------------------------------------------- */
 /* Workspace bytes a pyronn_cone_projection3d call with these arguments needs
- * (prepared geometry; for hardware_interp = 0 also two zero-padded copies of
- * one volume in the input dtype). */
+ * (prepared geometry; for hardware_interp = 0 also a copy of one volume as
+ * trilinear cells -- the 8 taps of each cell together -- and two zero-padded
+ * copies for views whose detector v axis does not run along z, all in the
+ * input dtype). */
 PYRONN_API size_t pyronn_cone_projection3d_workspace_size(int batch, int vol_z, int vol_y, int vol_x, int n_proj,
                                                           int det_h, int det_w, int in_dtype, int hardware_interp,
                                                           int geom_batch);
@@ -242,6 +244,54 @@ PYRONN_API int pyronn_cone_backprojection3d_noalloc(const void *sinogram, void *
                                                     const float *projection_matrices, const float *step_size,
                                                     const float *projection_multiplier, int geom_batch,
                                                     void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Geometry of circular trajectories, built on the device in FP64 on `stream`
+ * (no counterpart in the reference, whose ops receive these tensors from the
+ * PYRO-NN package, which builds them on the host): view n at angle
+ * start_angle + n * angular_range / n_proj.
+ *
+ * pyronn_circular_projection_matrices writes [n_proj, 3, 4] FP32 matrices P
+ * of a cone-beam scan: source at -SID (cos a, sin a, 0) mm, principal ray
+ * (cos a, sin a, 0), detector columns along (-sin a, cos a, 0), rows along +z,
+ * principal point (principal_v, principal_u) in pixel indices ((H-1)/2,
+ * (W-1)/2 for a centred detector); P maps world mm (x, y, z, 1) to
+ * (u w, v w, w) -- the projection_matrices input of the cone ops.
+ * pyronn_circular_ray_vectors_2d writes [n_proj, 2] FP32 (cos a, sin a), the
+ * ray_vectors / central_ray_vectors input of the 2D ops.
+ * ------------------------------------------------------------------------- */
+PYRONN_API int pyronn_circular_projection_matrices(float *projection_matrices, int n_proj, double sid, double sdd,
+                                                   double det_spacing_v, double det_spacing_u, double principal_v,
+                                                   double principal_u, double angular_range, double start_angle,
+                                                   void *stream);
+
+PYRONN_API int pyronn_circular_ray_vectors_2d(float *ray_vectors, int n_proj, double angular_range,
+                                              double start_angle, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * FDK / FBP pre-processing (no counterpart in the reference's ops; the
+ * PYRO-NN package filters in Python).  For every detector row of
+ * projections [batch, n_proj, det_h, det_w]:
+ *   g[k] = p[k] * SDD / sqrt(SDD^2 + u_k^2 + v^2)     (Feldkamp cosine weight;
+ *          u_k = (k - principal_u) * det_spacing_u, v = (row - principal_v) *
+ *          det_spacing_v; no weight when sdd == 0, i.e. parallel beam)
+ *   q[j] = tau * sum_k h[j - k] g[k]                   (linear convolution,
+ *          tau = det_spacing_u, h the Ram-Lak or Shepp-Logan ramp kernel of
+ *          Kak & Slaney ch. 3)
+ * weight_output = 1 applies the weight after the filter instead (the adjoint
+ * of the weight-then-filter operator, the kernel being symmetric).  FDK =
+ * this, then pyronn_cone_backprojection3d with projection_multiplier
+ * SID * SDD * pi / n_proj (full circle).  projections and filtered may be
+ * the same buffer.  det_w <= PYRONN_FDK_MAX_WIDTH.
+ * ------------------------------------------------------------------------- */
+#define PYRONN_FILTER_RAM_LAK 0
+#define PYRONN_FILTER_SHEPP_LOGAN 1
+#define PYRONN_FDK_MAX_WIDTH 4096
+
+PYRONN_API int pyronn_fdk_filter(const void *projections, void *filtered, int in_dtype, int out_dtype, int batch,
+                                 int n_proj, int det_h, int det_w, double sdd, double det_spacing_v,
+                                 double det_spacing_u, double principal_v, double principal_u, int filter,
+                                 int weight_output, void *stream);
 
 #ifdef __cplusplus
 }

@@ -275,3 +275,6 @@ def cone_backprojection3d_matched(sinogram, volume_shape, volume_origin, volume_
     lib().oracle_cone_backprojection3d_matched(_ptr(sino), _ptr(out), B, n_proj, H, W, Z, Y, X,
                                                *[_ptr(a) for a in args], g)
     return out
+
+
+from .filters import cosine_weights, fdk_filter, ramp_kernel  # noqa: E402,F401  (FDK / FBP pre-processing)

@@ -66,6 +66,11 @@ cudaError_t launch_cone_fp_padded(const void *volume, void *sinogram, int in_dty
                                   unsigned *flags, cudaStream_t stream);
 
 // matched (exact-adjoint) scatter backprojector (cone_matched.cu); FP32 output
+// FDK weighting + ramp filtering of `rows` detector rows (fdk.cu)
+cudaError_t launch_fdk_filter(const void *in, void *out, int in_dtype, int out_dtype, long long rows, int det_h,
+                              int W, float sdd, float dv, float du, float cv, float cu, int kind, int weight_output,
+                              cudaStream_t stream);
+
 cudaError_t launch_cone_scatter(const void *sinogram, float *volume, int in_dtype, const Dims3D &d,
                                 const ConeFpView *views, const float *step, const float *spacing,
                                 cudaStream_t stream);

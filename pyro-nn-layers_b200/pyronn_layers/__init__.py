@@ -11,6 +11,8 @@ They run hand-written sm_100a CUDA kernels through the C ABI of
 ``include/pyronn_b200.h`` (``libpyronn_b200.so`` in this directory).
 """
 from .ops import (  # noqa: F401
+    circular_projection_matrices,
+    circular_ray_vectors_2d,
     cone_backprojection3d,
     cone_backprojection3d_matched,
     cone_projection3d,
@@ -21,7 +23,7 @@ from .ops import (  # noqa: F401
     release_cached_arrays,
 )
 from ._capi import PyronnError  # noqa: F401
-from . import geometry, phantoms  # noqa: F401
+from . import fbp, geometry, phantoms  # noqa: F401
 
 __all__ = [
     "parallel_projection2d",
@@ -32,7 +34,10 @@ __all__ = [
     "cone_backprojection3d",
     "cone_backprojection3d_matched",
     "release_cached_arrays",
+    "circular_projection_matrices",
+    "circular_ray_vectors_2d",
     "PyronnError",
+    "fbp",
     "geometry",
     "phantoms",
 ]

@@ -27,6 +27,7 @@ ERROR_CUDA = 4
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _SZ = ctypes.c_size_t
+_D = ctypes.c_double
 
 # name -> (restype, argtypes); mirrors include/pyronn_b200.h
 PROTOTYPES = {
@@ -53,9 +54,15 @@ PROTOTYPES = {
         _I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _I, _P, _SZ, _P]),
     "pyronn_cone_backprojection3d_noalloc": (
         _I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _P]),
+    "pyronn_circular_projection_matrices": (_I, [_P, _I] + [_D] * 8 + [_P]),
+    "pyronn_circular_ray_vectors_2d": (_I, [_P, _I, _D, _D, _P]),
+    "pyronn_fdk_filter": (_I, [_P, _P, _I, _I, _I, _I, _I, _I] + [_D] * 5 + [_I, _I, _P]),
 }
 
 NOALLOC_MAX_VIEWS = 8192  # PYRONN_NOALLOC_MAX_VIEWS
+FILTER_RAM_LAK = 0  # PYRONN_FILTER_RAM_LAK
+FILTER_SHEPP_LOGAN = 1  # PYRONN_FILTER_SHEPP_LOGAN
+FDK_MAX_WIDTH = 4096  # PYRONN_FDK_MAX_WIDTH
 
 
 class PyronnError(RuntimeError):

@@ -23,6 +23,7 @@ mirrors ``REGISTER_OP("ConeProjection3D")`` (cc/ops/cone_projector_3D_OPKernel.c
 """
 from __future__ import annotations
 
+import math
 from typing import Sequence
 
 import torch
@@ -384,3 +385,33 @@ def cone_backprojection3d(sinogram, volume_shape, volume_origin, volume_spacing,
 def release_cached_arrays() -> None:
     """Frees the CUDA arrays the hardware_interp paths keep cached on the current device."""
     _capi.call("pyronn_release_cached_arrays")
+
+
+def circular_projection_matrices(n_proj: int, sid: float, sdd: float, detector_shape, detector_spacing,
+                                 angular_range: float = 2.0 * math.pi, start: float = 0.0, principal_point=None,
+                                 device="cuda") -> torch.Tensor:
+    """[n_proj, 3, 4] float32 projection matrices of a circular cone-beam scan,
+    built on `device` in FP64 (pyronn_circular_projection_matrices); the same
+    conventions and arguments as geometry.circular_projection_matrices, which
+    builds them on the host."""
+    H, W = int(detector_shape[0]), int(detector_shape[1])
+    cv, cu = ((H - 1) / 2.0, (W - 1) / 2.0) if principal_point is None else principal_point
+    dev = torch.device(device)
+    out = torch.empty((int(n_proj), 3, 4), dtype=torch.float32, device=dev)
+    with torch.cuda.device(dev):
+        _capi.call("pyronn_circular_projection_matrices", out.data_ptr(), int(n_proj), float(sid), float(sdd),
+                   float(detector_spacing[0]), float(detector_spacing[1]), float(cv), float(cu),
+                   float(angular_range), float(start), _stream(dev))
+    return out
+
+
+def circular_ray_vectors_2d(n_proj: int, angular_range: float = math.pi, start: float = 0.0,
+                            device="cuda") -> torch.Tensor:
+    """[n_proj, 2] float32 (cos, sin) ray vectors built on `device` in FP64
+    (pyronn_circular_ray_vectors_2d); geometry.ray_vectors_2d on the host."""
+    dev = torch.device(device)
+    out = torch.empty((int(n_proj), 2), dtype=torch.float32, device=dev)
+    with torch.cuda.device(dev):
+        _capi.call("pyronn_circular_ray_vectors_2d", out.data_ptr(), int(n_proj), float(angular_range), float(start),
+                   _stream(dev))
+    return out

@@ -122,3 +122,16 @@ def test_ops_refuse_cpu_tensors():
     geo = geometry.ConeBeam3D((8, 8, 8), (1, 1, 1), (8, 8), (1, 1), 4, 100, 150)
     with pytest.raises(ValueError, match="CUDA"):
         pl.cone_projection3d(torch.zeros(1, 8, 8, 8), geo.detector_shape, *geo.args())
+
+
+def test_trajectory_builders_reject_bad_arguments():
+    lib = _capi.load()
+    f = lib.pyronn_circular_projection_matrices
+    assert f(None, 4, 600.0, 1000.0, 1.0, 1.0, 1.0, 1.0, 6.28, 0.0, None) == _capi.ERROR_INVALID_ARGUMENT
+    assert f(FAKE, 0, 600.0, 1000.0, 1.0, 1.0, 1.0, 1.0, 6.28, 0.0, None) == _capi.ERROR_INVALID_ARGUMENT
+    assert f(FAKE, 4, -600.0, 1000.0, 1.0, 1.0, 1.0, 1.0, 6.28, 0.0, None) == _capi.ERROR_INVALID_ARGUMENT
+    assert b"positive" in lib.pyronn_last_error()
+    assert f(FAKE, 4, 600.0, 1000.0, 1.0, 1.0, float("nan"), 1.0, 6.28, 0.0, None) == _capi.ERROR_INVALID_ARGUMENT
+    g = lib.pyronn_circular_ray_vectors_2d
+    assert g(FAKE, -1, 3.14, 0.0, None) == _capi.ERROR_INVALID_ARGUMENT
+    assert g(FAKE, 4, float("inf"), 0.0, None) == _capi.ERROR_INVALID_ARGUMENT

@@ -106,9 +106,10 @@ def test_axis_aligned_rays(cuda):
 @pytest.mark.parametrize("fan", [False, True])
 @pytest.mark.parametrize("dtype", DTYPES)
 def test_2d_forward_layout_choice_is_bit_exact(cuda, fan, dtype):
-    """Views whose rays run along x read the transposed slice copy (given a
-    workspace); the taps are combined in the same order, so a result is the
-    same bits with and without the workspace, for every view direction."""
+    """Given a workspace, the forward reads bilinear cell copies (y-fastest
+    for views whose rays run along x); without one, the caller's slice with a
+    bounds test per tap.  The taps are combined in the same order, so a result
+    is the same bits either way, for every view direction."""
     if fan:
         geo, x = _fan_setup(cuda, dtype)
         fn = "pyronn_fan_projection2d"
@@ -420,3 +421,29 @@ def test_cone_projection_non_circular_views(cuda, dtype):
     out = pl.cone_projection3d(x, geo.detector_shape, *args, out_dtype=torch.float32)
     ref = oracle.cone_projection3d(rounded(x), geo.detector_shape, *args)
     assert rel_l2(out.cpu().numpy(), ref) < 2e-5
+
+
+# ------------------------------------------------------------ device geometry
+
+
+@pytest.mark.parametrize("start,rng_", [(0.0, 2 * math.pi), (0.3, math.pi + 0.4)])
+def test_device_geometry_matches_host_builder(cuda, start, rng_):
+    """The FP64 device builders give the host builder's matrices and ray
+    vectors (to FP32 rounding: CUDA's and the host's FP64 sin/cos may differ
+    in the last bit)."""
+    n, det, sp = 97, (40, 56), (1.3, 0.7)
+    host = geometry.circular_projection_matrices(n, 640.0, 1100.0, det, sp, rng_, start)
+    dev = pl.circular_projection_matrices(n, 640.0, 1100.0, det, sp, rng_, start, device=cuda)
+    np.testing.assert_allclose(dev.cpu().numpy(), host, rtol=2e-7, atol=2e-7 * np.abs(host).max())
+    rh = geometry.ray_vectors_2d(n, rng_, start)
+    rd = pl.circular_ray_vectors_2d(n, rng_, start, device=cuda)
+    np.testing.assert_allclose(rd.cpu().numpy(), rh, rtol=0, atol=1.2e-7)
+    # the device matrices drive the projector like the host ones
+    geo = geometry.ConeBeam3D((16, 20, 24), (1.0, 1.0, 1.0), det, sp, n, 640.0, 1100.0, rng_)
+    vol = phantoms.ellipsoid_phantom_3d(geo.volume_shape, geo.volume_spacing, seed=2, n=4)[0][None]
+    args = list(geo.args())
+    args[2] = host
+    a = pl.cone_projection3d(t(vol, cuda), geo.detector_shape, *args)
+    args[2] = dev
+    b = pl.cone_projection3d(t(vol, cuda), geo.detector_shape, *args)
+    assert rel_l2(b.cpu().numpy(), a.cpu().numpy()) < 1e-6
