@@ -595,13 +595,89 @@ def run_fan2d(args):
     print(json.dumps(line))
 
 
+def run_fdk(args):
+    """FDK of the 512^3 cone workload: cosine weighting + ramp filtering of the
+    360 x 768 x 1024 projections (storage dtype in, FP32 out) and the
+    backprojection of the filtered projections into an FP32 volume.  GUPS =
+    512^3 * 360 / t (the backprojection's updates over filter + backprojection
+    time); the filter is also reported as FP32 FLOP/s of the taps it
+    multiplies (Ram-Lak: the centre and the odd offsets, 2 FLOP each)."""
+    import math
+
+    import torch
+
+    from pyronn_layers import geometry, ops
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    cfg = WORKLOADS["cone512"]
+    storage = {"bf16": torch.bfloat16, "fp16": torch.float16, "fp32": torch.float32}[args.storage]
+    geo = geometry.ConeBeam3D(cfg["volume"], (cfg["voxel_mm"],) * 3, cfg["detector"], (cfg["pixel_mm"],) * 2,
+                              cfg["views"], cfg["sid_mm"], cfg["sdd_mm"], step_size=cfg["step_voxels"])
+    H, W = cfg["detector"]
+    n = cfg["views"]
+    rng = torch.Generator(device=dev).manual_seed(11)
+    sino = torch.rand((1, n, H, W), generator=rng, device=dev).to(storage)
+    q = torch.empty((1, n, H, W), dtype=torch.float32, device=dev)
+    vol = torch.empty((1,) + tuple(cfg["volume"]), dtype=torch.float32, device=dev)
+    gc = ops.GeometryCone(1, dev, geo.volume_origin, geo.volume_spacing, geo.projection_matrices, geo.step_size,
+                          np.array([geo.sid * geo.sdd * math.pi / n], np.float32), n)
+    ws = torch.empty(ops._capi.workspace_size("pyronn_cone_backprojection3d", 1, n, H, W, *cfg["volume"], 0, 0, 1),
+                     dtype=torch.uint8, device=dev)
+    code = ops.storage_code(storage)
+    ev = []
+
+    def step():
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        s = torch.cuda.current_stream(dev).cuda_stream
+        e[0].record()
+        ops._capi.call("pyronn_fdk_filter", sino.data_ptr(), q.data_ptr(), code, 0, 1, n, H, W, geo.sdd,
+                       cfg["pixel_mm"], cfg["pixel_mm"], (H - 1) / 2.0, (W - 1) / 2.0, 0, 0, s)
+        e[1].record()
+        ops._capi.call("pyronn_cone_backprojection3d", q.data_ptr(), vol.data_ptr(), 0, 0, 0, 1, n, H, W,
+                       *cfg["volume"], *gc.pointers(), 1, ws.data_ptr(), ws.numel(), s)
+        e[2].record()
+        ev.append(e)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    ev.clear()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(physical_gpu_index(dev.index or 0)) as clk:
+        t0.record()
+        for _ in range(args.steps):
+            step()
+        t1.record()
+        torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    f_ms = statistics.mean(a.elapsed_time(b) for a, b, _ in ev)
+    b_ms = statistics.mean(b.elapsed_time(c) for _, b, c in ev)
+    wp = (W + 15) // 16 * 16
+    flops = 2.0 * n * H * wp * (wp / 2 + 1)
+    line = {
+        "metric": "cone-beam FDK (filter + backprojection) GUPS", "value": updates(cfg) * args.steps / (ms / 1e3) / 1e9,
+        "unit": "GUPS", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "storage": args.storage, "data": "synthetic (uniform random projections)",
+        "config": {"workload": "fdk", "volume": list(cfg["volume"]), "views": n, "detector_hw": [H, W],
+                   "filter": "ram-lak", "filtered_storage": "fp32"},
+        "kernels": {"filter_ms": f_ms, "backprojection_ms": b_ms,
+                    "filter_tflops": flops / (f_ms / 1e3) / 1e12,
+                    "filter_note": "FP32 FMAs of the direct convolution over the nonzero Ram-Lak taps, "
+                                   "2 x rows x %d x (%d / 2 + 1) per launch" % (wp, wp)},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving", "fan2d"], default="cone512")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving", "fan2d", "fdk"], default="cone512")
     ap.add_argument("--requests", type=int, default=2000, help="serving: number of requests")
     ap.add_argument("--rate", type=float, default=100.0, help="serving: Poisson arrival rate (1/s)")
     ap.add_argument("--storage", choices=["bf16", "fp16", "fp32"], default="fp16",
@@ -621,6 +697,12 @@ def main(argv=None):
             print(json.dumps({"impl": "reference", "unavailable": "the fan2d workload is measured on the GPU arm only"}))
             return
         run_fan2d(args)
+        return
+    if args.workload == "fdk":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no FDK filter"}))
+            return
+        run_fdk(args)
         return
     if args.workload == "serving":
         if args.impl == "reference":

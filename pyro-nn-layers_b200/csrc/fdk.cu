@@ -13,9 +13,12 @@
 // consecutive outputs of one row with a sliding window of 16 taps in
 // registers: per input sample k, one tap load (the window's new element),
 // one broadcast load of g[k] and 16 FMAs.  The taps sit in shared memory with
-// one padding word per 32 (index i at i + i/32), which makes the lanes' tap
-// loads -- 16 apart -- fall in 32 distinct banks.  Results are staged
-// through shared memory so the rows are written coalesced.
+// one padding word per 16 (index i at i + i/16): the lanes' tap loads, 16
+// taps apart, land 17 words apart, in 32 distinct banks, and the 16 loads of
+// one window pass share one base address (immediate offsets).  Ram-Lak's
+// even taps are zero except the centre: its loop takes the odd taps only
+// (half the FMAs and tap loads) and adds the centre tap after.  Results are
+// staged through shared memory so the rows are written coalesced.
 #include "common.cuh"
 #include "internal.h"
 
@@ -25,9 +28,9 @@ namespace {
 
 constexpr int FB = 16;  // consecutive outputs per thread
 
-__device__ __forceinline__ int skew(int i)
+__host__ __device__ inline int skew(int i)
 {
-    return i + (i >> 5);
+    return i + (i >> 4);
 }
 
 __host__ __device__ inline int padded_width(int W)
@@ -44,11 +47,11 @@ __host__ __device__ inline int tap_count(int W)
 
 __host__ __device__ inline int tap_words(int W)
 {
-    const int n = tap_count(W);
-    return (n + (n >> 5) + 4) / 4 * 4;
+    return (skew(tap_count(W) - 1) + 1 + 3) / 4 * 4;
 }
 
-template <typename Tin, typename Tout>
+// ODD_ONLY: the Ram-Lak kernel, zero at every even offset but 0
+template <typename Tin, typename Tout, bool ODD_ONLY>
 __global__ void __launch_bounds__(256)
     fdk_filter_kernel(const Tin *in, Tout *out, long long rows, int det_h, int W,
                       float sdd, float dv, float du, float cv, float cu, int kind, int weight_output)
@@ -96,20 +99,32 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int a = 0; a < FB; ++a) acc[a] = 0.0f;
     if (j0 < Wp) {
-        // window slot (m mod FB) holds tap m; before the first step slots
-        // 1 .. FB-1 hold m = j0 + 1 .. j0 + FB - 1 (index m + Wp - 1)
+        // window slot (m mod FB) holds tap m (at index m + Wp - 1); before the
+        // first step slots 1 .. FB-1 hold m = j0 + 1 .. j0 + FB - 1.  Indices
+        // j0 + Wp + [0, 14] share i >> 4, so they are one base plus a.
+        const float *pre = taps + skew(j0 + Wp) - 1;
 #pragma unroll
-        for (int a = 1; a < FB; ++a) win[a] = taps[skew(j0 + a + Wp - 1)];
+        for (int a = 1; a < FB; ++a)
+            if (!ODD_ONLY || (a & 1)) win[a] = pre[a];
         for (int kk = 0; kk < Wp; kk += FB) {
+            // this pass's new taps m = j0 - kk - r, indices j0 - kk + Wp - 1 - r,
+            // r = 0 .. FB-1: one 16-aligned group, one base minus r
+            const float *tb = taps + skew(j0 - kk + Wp - 1);
 #pragma unroll
             for (int r = 0; r < FB; ++r) {
-                // step k = kk + r needs taps m = j0 - k + a; the new one (a = 0)
-                // goes into slot (-r) mod FB
-                win[(FB - r) % FB] = taps[skew(j0 - kk - r + Wp - 1)];
+                // step k = kk + r needs taps m = j0 - k + a; the new one (a = 0,
+                // parity of r) goes into slot (-r) mod FB
+                if (!ODD_ONLY || (r & 1)) win[(FB - r) % FB] = tb[-r];
                 const float gk = gr[kk + r];
 #pragma unroll
-                for (int a = 0; a < FB; ++a) acc[a] = fmaf(win[(a - r + FB) % FB], gk, acc[a]);
+                for (int a = 0; a < FB; ++a)
+                    if (!ODD_ONLY || ((a - r) & 1)) acc[a] = fmaf(win[(a - r + FB) % FB], gk, acc[a]);
             }
+        }
+        if (ODD_ONLY) {  // the centre tap, m = 0
+            const float h0 = taps[skew(Wp - 1)];
+#pragma unroll
+            for (int a = 0; a < FB; ++a) acc[a] = fmaf(h0, gr[j0 + a], acc[a]);
         }
     }
     __syncthreads();  // every thread is done with the row
@@ -145,11 +160,11 @@ cudaError_t launch_fdk_filter(const void *in, void *out, int in_dtype, int out_d
     return dispatch_dtypes(in_dtype, out_dtype, [&](auto tin, auto tout) -> cudaError_t {
         using Tin = typename decltype(tin)::type;
         using Tout = typename decltype(tout)::type;
-        cudaError_t e = cudaFuncSetAttribute(fdk_filter_kernel<Tin, Tout>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        auto kernel = kind == 0 ? fdk_filter_kernel<Tin, Tout, true> : fdk_filter_kernel<Tin, Tout, false>;
+        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        fdk_filter_kernel<Tin, Tout><<<(unsigned)blocks, dim3(tpr, rpb), smem, stream>>>(
-            (const Tin *)in, (Tout *)out, rows, det_h, W, sdd, dv, du, cv, cu, kind, weight_output);
+        kernel<<<(unsigned)blocks, dim3(tpr, rpb), smem, stream>>>((const Tin *)in, (Tout *)out, rows, det_h, W,
+                                                                  sdd, dv, du, cv, cu, kind, weight_output);
         return cudaGetLastError();
     });
 }
