@@ -493,11 +493,17 @@ def run_serving(args):
     geos = serving.standard_geometries()
     trace = serving.poisson_trace(args.requests, args.rate, seed=7)
     jobs = serving.make_jobs(trace, geos, seed=1)
-    # warm-up: one of each class through the server (graphs, caches, lazy set-up)
-    warm = serving.make_jobs([(0.0, c) for c in sorted({c for _, c in trace}, key=str)], geos, seed=1)
+    # start-up: buffer sets and graphs of batch sizes 1 and 2 for every class
+    # (a server does this before taking requests), then one job of each class
+    # through both paths so lazy set-up is out of the timed traces
+    classes = sorted({c for _, c in trace}, key=str)
     server = serving.ProjectorServer(geos, device=dev, keep_results=False)
+    warmup_s = server.warmup(classes, batch_sizes=(1, 2))
+    warm = serving.make_jobs([(0.0, c) for c in classes], geos, seed=1)
     server.run_trace(warm, realtime=False)
     server.batches, server.batch_sizes = 0, []
+    serving.run_plain(serving.make_jobs([(0.0, c) for c in classes], geos, seed=1), geos, device=dev,
+                      realtime=False)
     with ClockSampler(physical_gpu_index(dev.index or 0)) as clk:
         s_srv = server.run_trace(jobs, realtime=True)
     jobs_plain = serving.make_jobs(trace, geos, seed=1)
@@ -511,6 +517,7 @@ def run_serving(args):
                           "(360 views, 512^2); forward/back 50/50; FP32/BF16 50/50",
                    "arrivals": "Poisson, seed 7"},
         "serving": s_srv.as_dict(),
+        "server_startup_s": warmup_s,
         "plain_one_job_per_launch_fp32": s_plain.as_dict(),
         "clocks": clk.summary(),
     }

@@ -314,18 +314,18 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
+// looked up once per process (a function-local static initialises once, also
+// when several host threads get here together)
 EncodeTiledFn encode_fn()
 {
-    static EncodeTiledFn fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
+    static const EncodeTiledFn fn = []() -> EncodeTiledFn {
         void *p = nullptr;
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = (EncodeTiledFn)p;
-    }
+            return (EncodeTiledFn)p;
+        return nullptr;
+    }();
     return fn;
 }
 
@@ -367,13 +367,11 @@ cudaError_t launch_typed(const void *sinogram, void *volume, const Dims3D &d, co
     const dim3 grid((d.vol_x + TB_X - 1) / TB_X, (d.vol_y + TB_Y - 1) / TB_Y, zblocks * d.batch);
     static_assert((BOX_ELEMS * sizeof(float)) % 128 == 0 && (BOX_ELEMS * 2) % 128 == 0, "tile alignment");
     const size_t smem = 2 * BP_K * BOX_ELEMS * sizeof(Tin) + 128;
-    static bool attr_set = false;  // per instantiation
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(cone_bp_tma_kernel<Tin, Tout>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
+    // set on every launch: the attribute belongs to the current device's copy
+    // of the kernel, and the call is a cheap host-side update
+    cudaError_t e = cudaFuncSetAttribute(cone_bp_tma_kernel<Tin, Tout>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
     cone_bp_tma_kernel<Tin, Tout><<<grid, block, smem, stream>>>(map, (const Tin *)sinogram, (Tout *)volume, views, mult,
                                                                d.vol_x, d.vol_y, d.vol_z, d.det_w, d.det_h, d.n_proj,
                                                                d.geom_batch, err);

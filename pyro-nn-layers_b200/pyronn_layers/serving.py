@@ -175,6 +175,7 @@ class Executor:
         self._sets = {}      # set -> (inp, out, ws)
         self._graphs = {}    # (batch, set) -> torch.cuda.CUDAGraph
         self._runs = {}      # (batch, set) -> eager runs so far
+        self._cap = None     # side stream for graph captures
         self.graph_replays = 0
         g = entry.geo
         if entry.kind == "fan":
@@ -274,15 +275,37 @@ class Executor:
         n = self._runs.get(key, 0) + 1
         self._runs[key] = n
         if self.use_graphs and n >= 2:
-            # capture after a warm-up run (lazy one-time set-up happens eagerly);
-            # the replay is recorded on a side stream ordered after this batch
+            # capture after a warm-up run (lazy one-time set-up happens
+            # eagerly), on a side stream ordered after this batch.  The launch
+            # sequence allocates nothing, so the capture needs none of the
+            # device-wide synchronisation, garbage collection and cache
+            # flush that torch.cuda.graph() performs on entry -- in a serving
+            # loop those stall every stream for the length of the longest
+            # batch in flight.
             g = t.cuda.CUDAGraph()
-            cap = t.cuda.Stream(self.device)
+            cap = self._capture_stream()
             cap.wait_stream(stream)
-            with t.cuda.graph(g, stream=cap):
-                self._launch(batch, bset, t.cuda.current_stream(self.device).cuda_stream)
+            with t.cuda.stream(cap):
+                g.capture_begin()
+                try:
+                    self._launch(batch, bset, cap.cuda_stream)
+                finally:
+                    g.capture_end()
             stream.wait_stream(cap)
             self._graphs[key] = g
+
+    def _capture_stream(self):
+        if self._cap is None:
+            self._cap = self.torch.cuda.Stream(self.device)
+        return self._cap
+
+    def prepare(self, batch: int, stream) -> None:
+        """Allocates every buffer set and records the graphs of a batch size
+        (two eager runs per set; results are not meaningful)."""
+        for bset in range(self.n_sets):
+            self.allocate(bset)
+            while self.use_graphs and (batch, bset) not in self._graphs:
+                self.run(batch, bset, stream)
 
 
 class ProjectorServer:
@@ -312,6 +335,21 @@ class ProjectorServer:
             self.executors[cls] = Executor(cls, self.geometries[cls.geometry], self.device, self.max_batch,
                                            self.use_graphs)
         return self.executors[cls]
+
+    def warmup(self, classes, batch_sizes=(1,)) -> float:
+        """Start-up work a server does before taking requests: the buffer sets
+        of each class and the graphs of the given batch sizes, so that first
+        requests do not pay allocation and capture.  Returns the seconds it
+        took."""
+        t0 = time.perf_counter()
+        stream = self.streams[0]
+        for cls in classes:
+            ex = self.executor(cls)
+            for b in batch_sizes:
+                if b <= self.max_batch:
+                    ex.prepare(b, stream)
+        self.torch.cuda.synchronize(self.device)
+        return time.perf_counter() - t0
 
     def free_hbm(self) -> int:
         """Free device memory, counting what torch's allocator holds unused."""
