@@ -14,7 +14,9 @@ backprojection, used for both directions as the metric defines it).
   data-path collective).
 * ``e2e``: the same step through the public API (pyronn_layers ops) with the
   volume copied from pinned host memory and the result copied back inside the
-  timed region.
+  timed region, steps pipelined over two slots as a stream of volumes runs
+  (the next input's upload and the last result's download overlap a step's
+  projections).
 * ``roofline``: the dominant kernel's algorithmic gather bytes (8 taps per
   forward ray sample, 4 taps per backprojection update, times the storage
   element size, plus its output bytes) over its live CUDA-event time, against
@@ -399,20 +401,61 @@ def run_ours(args, cfg):
         del step32
         torch.cuda.empty_cache()
 
-    # ---- end to end through the public API: pinned host volume in, volume out
-    host_in = torch.empty((1, Z, Y, X), dtype=storage, pin_memory=True)
-    host_in.copy_(x.cpu())
-    host_out = torch.empty((1, Z, Y, X), dtype=torch.float32, pin_memory=True)
+    # ---- end to end through the public API: pinned host volume in, FP32
+    # volume out, every step.  Steps run as a stream of volumes does: two
+    # slots, the host->device copy of step i+1 and the device->host copy of
+    # step i overlap step i's projections (copy engines, own streams); the
+    # timed region ends when the last result is in host memory.
+    host_in = [torch.empty((1, Z, Y, X), dtype=storage, pin_memory=True) for _ in range(2)]
+    for h in host_in:
+        h.copy_(x.cpu())
+    host_out = [torch.empty((1, Z, Y, X), dtype=torch.float32, pin_memory=True) for _ in range(2)]
+    dev_in = [torch.empty_like(x) for _ in range(2)]
+    h2d, d2h = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    comp = torch.cuda.current_stream(dev)
+    slot_done = [None, None]
     args_geo = geo.args()
 
-    def e2e_step(rec=False):
-        xd = host_in.to(dev, non_blocking=True)
-        s = pl.cone_projection3d(xd, geo.detector_shape, *args_geo, hardware_interp=hw, out_dtype=sino_storage)
-        b = pl.cone_backprojection3d(s, geo.volume_shape, *args_geo, hardware_interp=hw, out_dtype=torch.float32)
-        host_out.copy_(b, non_blocking=True)
+    def e2e_run(n):
+        for i in range(n):
+            k = i % 2
+            with torch.cuda.stream(h2d):
+                if slot_done[k] is not None:
+                    h2d.wait_event(slot_done[k])  # step i-2 is done reading the slot
+                dev_in[k].copy_(host_in[k], non_blocking=True)
+                ev_in = torch.cuda.Event()
+                ev_in.record(h2d)
+            comp.wait_event(ev_in)
+            s = pl.cone_projection3d(dev_in[k], geo.detector_shape, *args_geo, hardware_interp=hw,
+                                     out_dtype=sino_storage)
+            b = pl.cone_backprojection3d(s, geo.volume_shape, *args_geo, hardware_interp=hw,
+                                         out_dtype=torch.float32)
+            ev_b = torch.cuda.Event()
+            ev_b.record(comp)
+            slot_done[k] = ev_b
+            with torch.cuda.stream(d2h):
+                d2h.wait_event(ev_b)
+                host_out[k].copy_(b, non_blocking=True)
+                b.record_stream(d2h)
 
-    e2e_steps = max(2, min(args.steps, 5))
-    e2e_ms = timed(e2e_step, e2e_steps, min(args.warmup, 3), None)
+    e2e_steps = max(4, min(args.steps, 8))
+    e2e_run(max(args.warmup, 3))
+    torch.cuda.synchronize()
+    barrier()
+    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_start.record(comp)
+    h2d.wait_stream(comp)
+    e2e_run(e2e_steps)
+    comp.wait_stream(h2d)
+    comp.wait_stream(d2h)
+    e_end.record(comp)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = e_start.elapsed_time(e_end)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
     e2e_value = 2 * updates(cfg) * world * e2e_steps / (e2e_ms / 1e3) / 1e9
 
     # ---- roofline of the dominant kernel
@@ -449,8 +492,13 @@ def run_ours(args, cfg):
                     "forward_gsamples_per_s": S / (f_ms / 1e3) / 1e9,
                     "backprojection_gups": updates(cfg) / (b_ms / 1e3) / 1e9},
         "roofline": roofline,
-        "e2e": {"value": e2e_value, "unit": "GUPS", "h2d_bytes_per_step": host_in.numel() * host_in.element_size(),
-                "d2h_bytes_per_step": host_out.numel() * host_out.element_size(), "steps": e2e_steps},
+        "e2e": {"value": e2e_value, "unit": "GUPS",
+                "h2d_bytes_per_step": host_in[0].numel() * host_in[0].element_size(),
+                "d2h_bytes_per_step": host_out[0].numel() * host_out[0].element_size(), "steps": e2e_steps,
+                "api": "pyronn_layers.cone_projection3d + cone_backprojection3d",
+                "overlap": "two slots: the H2D copy of step i+1 and the D2H copy of step i run on their own "
+                           "streams during step i's projections; every step's input and result cross the host "
+                           "link inside the timed region"},
         "gpu_launches": LAUNCHES_PER_STEP[hw] * args.steps,
         "clocks": clocks,
     }
