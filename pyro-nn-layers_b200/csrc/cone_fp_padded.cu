@@ -281,7 +281,8 @@ struct ClampedCellSampler {
 // block's 8 x 32 results go through shared memory so the sinogram rows are
 // written 8 pixels at a time; xy mode: a warp is 32 consecutive u.
 template <typename T, typename Tout>
-__global__ void __launch_bounds__(PB_X *PB_Y)
+// (at least 3 blocks per SM: room for the 4-sample loop's registers)
+__global__ void __launch_bounds__(PB_X *PB_Y, 3)
     cone_fp_padded_kernel(const T *__restrict__ xfast, const T *__restrict__ yfast,
                           const typename Cell<T>::type *__restrict__ cells, Tout *__restrict__ sino,
                           const ConeFpView *__restrict__ views, const float *__restrict__ step_ptr,
@@ -315,7 +316,7 @@ __global__ void __launch_bounds__(PB_X *PB_Y)
             const int Yc = Y + 2, Zc = Z + 2;
             const CellSampler<T> s(cells + (Yc + 1) * Zc + 1, Zc, Yc * Zc);
             const int n = inside ? exact_sample_count(ray, step) : -1;
-            pixel = n > 0    ? march_counted_x2(ray, n, step, s)
+            pixel = n > 0    ? march_counted_x4(ray, n, step, s)
                     : inside ? march_x2(ray, step, s)
                              : march_x2(ray, step, ClampedCellSampler<T>{s, xmax, ymax, zmax});
         } else {

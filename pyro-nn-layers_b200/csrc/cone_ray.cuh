@@ -216,6 +216,53 @@ __device__ __forceinline__ float march_counted_x2(const ConeRay &ray, int n, flo
     return pixel * ray.mm_scale;
 }
 
+// march_counted_x2 with four samples per iteration (their four cell loads in
+// flight together): the same samples, alpha sequence and order of additions.
+template <typename F>
+__device__ __forceinline__ float march_counted_x4(const ConeRay &ray, int n, float step, const F &sample)
+{
+    float a = ray.a;
+    float px = fmaf(a, ray.dx, ray.ox), py = fmaf(a, ray.dy, ray.oy), pz = fmaf(a, ray.dz, ray.oz);
+    float pixel = 0.5f * sample(px, py, pz);
+    a += step;
+    int k = 1;
+    for (; k + 3 < n; k += 4) {
+        const float a1 = a + step, a2 = a1 + step, a3 = a2 + step;
+        const float v0 = sample(fmaf(a, ray.dx, ray.ox), fmaf(a, ray.dy, ray.oy), fmaf(a, ray.dz, ray.oz));
+        const float v1 = sample(fmaf(a1, ray.dx, ray.ox), fmaf(a1, ray.dy, ray.oy), fmaf(a1, ray.dz, ray.oz));
+        const float v2 = sample(fmaf(a2, ray.dx, ray.ox), fmaf(a2, ray.dy, ray.oy), fmaf(a2, ray.dz, ray.oz));
+        px = fmaf(a3, ray.dx, ray.ox);
+        py = fmaf(a3, ray.dy, ray.oy);
+        pz = fmaf(a3, ray.dz, ray.oz);
+        const float v3 = sample(px, py, pz);
+        pixel += v0;
+        pixel += v1;
+        pixel += v2;
+        pixel += v3;
+        a = a3 + step;
+    }
+    for (; k < n; ++k) {
+        px = fmaf(a, ray.dx, ray.ox);
+        py = fmaf(a, ray.dy, ray.oy);
+        pz = fmaf(a, ray.dz, ray.oz);
+        pixel += sample(px, py, pz);
+        a += step;
+    }
+    pixel *= step;
+    if (pixel > 0.0f) {
+        const float last_val = sample(px, py, pz);
+        pixel -= 0.5f * step * last_val;
+        a -= step;
+        const float last_step = ray.am - a;
+        pixel += 0.5f * last_step * last_val;
+        px = fmaf(ray.am, ray.dx, ray.ox);
+        py = fmaf(ray.am, ray.dy, ray.oy);
+        pz = fmaf(ray.am, ray.dz, ray.oz);
+        pixel += 0.5f * last_step * sample(px, py, pz);
+    }
+    return pixel * ray.mm_scale;
+}
+
 // Number of samples of the march when its float alpha sequence is exact:
 // step a multiple of ulp(a0) and every alpha up to the one after the last
 // sample below the next power of two above a0, so each a += step adds
