@@ -447,3 +447,53 @@ def test_device_geometry_matches_host_builder(cuda, start, rng_):
     args[2] = dev
     b = pl.cone_projection3d(t(vol, cuda), geo.detector_shape, *args)
     assert rel_l2(b.cpu().numpy(), a.cpu().numpy()) < 1e-6
+
+
+# ------------------------------------------------------------ degenerate sizes
+
+
+@pytest.mark.parametrize("vol_shape,det,n_proj,batch", [
+    ((1, 1, 1), (1, 1), 1, 1),      # one voxel, one pixel, one view
+    ((3, 5, 7), (2, 3), 3, 3),      # ragged odd sizes, batch of 3
+    ((9, 1, 4), (5, 1), 2, 2),      # flat volume, one-column detector
+])
+@pytest.mark.parametrize("hw", [False, True])
+def test_cone_tiny_and_ragged_shapes(cuda, vol_shape, det, n_proj, batch, hw):
+    """Every cone path on sizes far below one tile or one TMA box, against the
+    oracle: partial blocks, single views and one-pixel detectors."""
+    geo = geometry.ConeBeam3D(vol_shape, (1.0, 0.9, 1.1), det, (1.2, 1.3), n_proj, 60.0, 100.0, step_size=0.5)
+    rng = np.random.Generator(np.random.PCG64(31))
+    vol = rng.uniform(0.2, 1.0, (batch,) + vol_shape).astype(np.float32)
+    out = pl.cone_projection3d(t(vol, cuda), geo.detector_shape, *geo.args(), hardware_interp=hw)
+    ref = oracle.cone_projection3d(vol, geo.detector_shape, *geo.args(), hardware_interp=hw)
+    tol = 5e-3 if hw else 2e-5
+    assert out.shape == (batch,) + geo.detector_shape
+    assert rel_l2(out.cpu().numpy(), ref) < tol or np.abs(ref).max() == 0
+    sino = rng.uniform(0.2, 1.0, (batch,) + geo.detector_shape).astype(np.float32)
+    back = pl.cone_backprojection3d(t(sino, cuda), geo.volume_shape, *geo.args(), hardware_interp=hw)
+    refb = oracle.cone_backprojection3d(sino, geo.volume_shape, *geo.args(), hardware_interp=hw)
+    assert back.shape == (batch,) + vol_shape
+    assert rel_l2(back.cpu().numpy(), refb) < (5e-3 if hw else 1e-5) or np.abs(refb).max() == 0
+
+
+@pytest.mark.parametrize("vol_shape,det_w,n_proj,batch", [((1, 1), 1, 1, 1), ((5, 3), 7, 2, 3), ((2, 33), 4, 5, 1)])
+@pytest.mark.parametrize("fan", [False, True])
+def test_2d_tiny_and_ragged_shapes(cuda, vol_shape, det_w, n_proj, batch, fan):
+    if fan:
+        geo = geometry.FanBeam2D(vol_shape, (1.0, 0.8), det_w, 1.1, n_proj, 40.0, 70.0)
+        fwd, bwd, ofwd, obwd = (pl.fan_projection2d, pl.fan_backprojection2d, oracle.fan_projection2d,
+                                oracle.fan_backprojection2d)
+    else:
+        geo = geometry.ParallelBeam2D(vol_shape, (1.0, 0.8), det_w, 1.1, n_proj)
+        fwd, bwd, ofwd, obwd = (pl.parallel_projection2d, pl.parallel_backprojection2d, oracle.parallel_projection2d,
+                                oracle.parallel_backprojection2d)
+    rng = np.random.Generator(np.random.PCG64(32))
+    img = rng.uniform(0.2, 1.0, (batch,) + vol_shape).astype(np.float32)
+    out = fwd(t(img, cuda), geo.detector_shape, *geo.args())
+    ref = ofwd(img, geo.detector_shape, *geo.args())
+    assert out.shape == (batch,) + geo.detector_shape
+    assert rel_l2(out.cpu().numpy(), ref) < 2e-5 or np.abs(ref).max() == 0
+    sino = rng.uniform(0.2, 1.0, (batch,) + geo.detector_shape).astype(np.float32)
+    back = bwd(t(sino, cuda), geo.volume_shape, *geo.args())
+    refb = obwd(sino, geo.volume_shape, *geo.args())
+    assert rel_l2(back.cpu().numpy(), refb) < 1e-5 or np.abs(refb).max() == 0
