@@ -179,7 +179,7 @@ def _run_2d(forward: bool, x: torch.Tensor, out_dims, geo: Geometry2D, out_dtype
         out = torch.empty((batch, n_proj, det_w), dtype=od, device=dev)
         fn = "pyronn_fan_projection2d" if geo.fan else "pyronn_parallel_projection2d"
         dims = [batch, vol_y, vol_x, n_proj, det_w]
-        # the transposed slice copy read by views whose rays run along x
+        # workspace for the x- and y-fastest bilinear cell copies of the batch
         ws_bytes = _capi.workspace_size("pyronn_projection2d", batch, vol_y, vol_x, storage_code(x.dtype))
         if workspace is None or workspace.numel() < ws_bytes:
             workspace = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
