@@ -20,10 +20,11 @@
 // outside the detector contributes zero and is skipped.
 //
 // Views whose u and w rows have a zero z coefficient -- every view of a
-// circular trajectory about the z axis -- take a column loop: 1/w, u, the u
-// tap and its weight are then the same for the thread's 16 voxels and are
-// computed once; the values are exactly those of the general loop, so is the
-// result.
+// circular trajectory about the z axis -- take a column loop: 1/w, w^-2, u,
+// the u tap and its weight are then the same for the thread's 16 voxels and
+// are computed once, and v steps along the column as one FMA from its value
+// at the column base (within a few ulp of the general loop's per-voxel
+// v = (P1 . x) / w).
 #include <cuda.h>
 
 #include "common.cuh"
@@ -247,16 +248,15 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
             if (mode == MODE_SMEM && m.zconst) {
                 const T *tile = &tiles[cur][k][0];
                 // fmaf(0, z, x) == x: these are the general loop's values at every z
-                const float rw = fast_rcp(wb);
+                const float rw = fast_rcp(wb), rw2 = rw * rw;
                 const FloorFrac fu = floor_frac(ub * rw - m.u0);
                 const float tx = fu.f;
                 // row of floor(lv) from its FloorFrac bits: the bias folded into one offset
                 const unsigned col = (unsigned)fu.i - (unsigned)FLOOR_BIAS * (unsigned)BOX_W;
-                const float v0 = m.v0;
+                const float lv0 = fmaf(vb, rw, -m.v0), dlv = r1.z * rw;  // local v at z = 0, its step
 #pragma unroll
                 for (int z = 0; z < TB_Z; ++z) {
-                    const float fz = (float)z;
-                    const float lv = fmaf(r1.z, fz, vb) * rw - v0;
+                    const float lv = fmaf((float)z, dlv, lv0);
                     const FloorFrac fv = floor_frac(lv);
                     unsigned idx = (unsigned)fv.bits * (unsigned)BOX_W + col;
                     idx = min(idx, MAX_IDX);  // memory safety only: the margin keeps idx in range
@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
                     const float p10 = smem_to_float(tile + idx + BOX_W);
                     const float p11 = smem_to_float(tile + idx + BOX_W + 1);
                     const float val = lerp_ref(lerp_ref(p00, p01, tx), lerp_ref(p10, p11, tx), fv.f);
-                    acc[z] = fmaf(val * rw, rw, acc[z]);
+                    acc[z] = fmaf(val, rw2, acc[z]);
                 }
             } else if (mode == MODE_SMEM) {
                 const T *tile = &tiles[cur][k][0];
