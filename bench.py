@@ -149,7 +149,7 @@ class ClockSampler:
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,utilization.gpu")
 
     def __init__(self, gpu_index):
         self.gpu_index = gpu_index
@@ -183,12 +183,18 @@ class ClockSampler:
     def summary(self):
         if not getattr(self, "rows", None):
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        # the SM clock under load: samples whose utilisation is at least 50 %
+        # (the sampler also sees set-up and host-side gaps, where the clock idles)
+        def num(x):
+            return x.replace(".", "").isdigit()
+
+        loaded = [r for r in self.rows if len(r) > 9 and num(r[9]) and float(r[9]) >= 50.0]
+        sm = [float(r[1]) for r in (loaded or self.rows) if num(r[1])]
+        smax = [float(r[2]) for r in self.rows if num(r[2])]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": reasons, "samples": len(self.rows),
+                "reasons": reasons, "samples": len(self.rows), "samples_under_load": len(loaded),
                 "power_w_max": max(float(r[3]) for r in self.rows if r[3].replace(".", "").isdigit())
                 if any(r[3].replace(".", "").isdigit() for r in self.rows) else None}
 

@@ -141,9 +141,9 @@ struct ClampedCellSampler2 {
 };
 
 // The ray march of kernel_project2D (par_projector_2D_CudaKernel.cu.cc:58-102)
-// at positions (bx + a gx, by + a gy) in index space, two samples per
-// iteration (their gathers overlap) with the same alpha sequence and order of
-// additions as one at a time.
+// at positions (bx + a gx, by + a gy) in index space, four (then two, then
+// one) samples per iteration (their gathers overlap) with the same alpha
+// sequence and order of additions as one at a time.
 template <typename F>
 __device__ __forceinline__ float march2d(float a, float am, float step, float gx, float bx, float gy, float by,
                                          const F &sample)
@@ -158,6 +158,24 @@ __device__ __forceinline__ float march2d(float a, float am, float step, float gx
         pixel += 0.5f * sample(px, py);
         a += step;
         ++iter;
+    }
+    // four samples per compare while the fourth alpha is still before the
+    // exit (the sequence never decreases, so the first three are too)
+    while (iter + 3 < max_iter) {
+        const float a1 = a + step, a2 = a1 + step, a3 = a2 + step;
+        if (!(a3 < am)) break;
+        const float v0 = sample(fmaf(a, gx, bx), fmaf(a, gy, by));
+        const float v1 = sample(fmaf(a1, gx, bx), fmaf(a1, gy, by));
+        const float v2 = sample(fmaf(a2, gx, bx), fmaf(a2, gy, by));
+        px = fmaf(a3, gx, bx);
+        py = fmaf(a3, gy, by);
+        const float v3 = sample(px, py);
+        pixel += v0;
+        pixel += v1;
+        pixel += v2;
+        pixel += v3;
+        a = a3 + step;
+        iter += 4;
     }
     while (a < am && iter < max_iter) {
         const float a1 = a + step;

@@ -48,3 +48,15 @@ def test_two_gloo_ranks_max_time_and_distinct_shards():
 def test_updates_of_workloads():
     assert bench.updates(bench.WORKLOADS["cone512"]) == 48318382080
     assert bench.updates(bench.WORKLOADS["cone256"]) == 6039797760
+
+
+def test_clock_summary_uses_samples_under_load():
+    """The reported SM clock is the median over samples taken under load; a
+    throttle reason seen in any sample is reported."""
+    c = bench.ClockSampler(0)
+    idle = ["0", "345", "1965", "90", "0x0", "Not Active", "Not Active", "Not Active", "Not Active", "0"]
+    busy = ["0", "1965", "1965", "700", "0x0", "Not Active", "Not Active", "Not Active", "Active", "100"]
+    c.rows = [idle, busy, busy, idle, idle]
+    s = c.summary()
+    assert s["sm_mhz"] == 1965.0 and s["samples_under_load"] == 2
+    assert s["reasons"] == ["sw_power_cap"]
