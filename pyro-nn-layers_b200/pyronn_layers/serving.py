@@ -330,6 +330,17 @@ class ProjectorServer:
         self.batches = 0
         self.batch_sizes = []
 
+    def register_geometry(self, name: str, descriptor: dict) -> GeometryEntry:
+        """Adds a geometry from its wire descriptor (wire.geometry_descriptor
+        or wire.circular_descriptor) under name; requests refer to it."""
+        from . import wire
+        if name in self.geometries:
+            raise ValueError("geometry %r is already registered" % (name,))
+        kind, geo = wire.geometry_from_descriptor(descriptor)
+        entry = GeometryEntry(kind, geo, geo.volume_shape, geo.detector_shape)
+        self.geometries[name] = entry
+        return entry
+
     def executor(self, cls: JobClass) -> Executor:
         if cls not in self.executors:
             self.executors[cls] = Executor(cls, self.geometries[cls.geometry], self.device, self.max_batch,
@@ -495,6 +506,40 @@ def run_plain(jobs: List[Job], geometries: Dict[str, GeometryEntry], device=None
     wall = clock() - t0
     lat = np.array([(j.done - j.arrival) * 1e3 for j in jobs])
     return ServeStats(lat, percentile(lat, 50), percentile(lat, 99), total / wall / 1e9, wall, len(jobs), 1.0, 0)
+
+
+def job_from_request(req: dict, geometries: Dict[str, GeometryEntry], arrival: float = 0.0) -> Job:
+    """A Job from a decoded wire request (wire.decode_request): the input in
+    pinned host memory in its storage dtype, checked against the geometry."""
+    import torch
+    entry = geometries.get(req["geometry"])
+    if entry is None:
+        raise KeyError("unknown geometry %r" % (req["geometry"],))
+    kind, direction = req["op"].split("_")
+    if kind != entry.kind:
+        raise ValueError("op %s on a %s geometry" % (req["op"], entry.kind))
+    shape = entry.volume_shape if direction == "fwd" else entry.sinogram_shape
+    data = np.asarray(req["data"])
+    if tuple(data.shape) != tuple(shape):
+        raise ValueError("input of shape %s, the geometry needs %s" % (data.shape, tuple(shape)))
+    if req["dtype"] == "bf16":
+        t = torch.from_numpy(data.astype(np.int16, copy=False)).view(torch.bfloat16)
+    else:
+        t = torch.from_numpy(np.array(data, copy=True))
+    t = t.contiguous().pin_memory()
+    return Job(int(req["id"]), JobClass(req["op"], req["geometry"], req["dtype"]), t, arrival, entry.updates)
+
+
+def result_message(job: Job) -> bytes:
+    """The job's result (device or host tensor) as a wire result message, in
+    the dtype the server produced (FP32 volumes for backprojections)."""
+    import torch
+    from . import wire
+    r = job.result.detach().cpu().contiguous()
+    if r.dtype == torch.bfloat16:
+        return wire.encode_result(job.id, "bf16", r.view(torch.int16).numpy().view(np.uint16))
+    name = {torch.float32: "fp32", torch.float16: "fp16"}[r.dtype]
+    return wire.encode_result(job.id, name, r.numpy())
 
 
 def make_jobs(trace, geometries: Dict[str, GeometryEntry], seed: int = 0, pin: bool = True) -> List[Job]:

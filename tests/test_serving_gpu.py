@@ -61,3 +61,41 @@ def test_graphs_are_replayed_and_memory_is_admitted(cuda):
     tight = serving.ProjectorServer(geos, device=cuda, hbm_reserve=1 << 50)
     with pytest.raises(MemoryError):
         tight.run_trace(serving.make_jobs(trace[:2], geos, seed=2), realtime=False)
+
+
+def test_wire_requests_through_the_server(cuda):
+    """Geometries registered from wire descriptors and jobs decoded from wire
+    requests give, as wire results, the same arrays as the ops called directly."""
+    from pyronn_layers import wire
+    server = serving.ProjectorServer({}, device=cuda, max_batch=2)
+    server.register_geometry("cone-a", wire.circular_descriptor("cone", (24, 24, 24), (1.0, 1.0, 1.0), (32, 40),
+                                                                (1.5, 1.5), 20, 120.0, 200.0))
+    fan = geometry.FanBeam2D((64, 64), (0.5, 0.5), 128, 0.5, 60, 75.0, 120.0)
+    server.register_geometry("fan-b", wire.geometry_descriptor("fan", fan))
+    with pytest.raises(ValueError):
+        server.register_geometry("fan-b", wire.geometry_descriptor("fan", fan))
+    rng = np.random.Generator(np.random.PCG64(9))
+    reqs = []
+    for i, (op, name, dtype) in enumerate([("cone_fwd", "cone-a", "fp32"), ("cone_bp", "cone-a", "fp16"),
+                                            ("fan_fwd", "fan-b", "bf16"), ("fan_bp", "fan-b", "fp32"),
+                                            ("cone_fwd", "cone-a", "fp32")]):
+        e = server.geometries[name]
+        shape = e.volume_shape if op.endswith("fwd") else e.sinogram_shape
+        x = torch.as_tensor(rng.uniform(0, 1, shape), dtype={"fp32": torch.float32, "fp16": torch.float16,
+                                                              "bf16": torch.bfloat16}[dtype])
+        payload = x.view(torch.int16).numpy().view(np.uint16) if dtype == "bf16" else x.numpy()
+        reqs.append((wire.encode_request(i, op, name, dtype, payload), x))
+    jobs = [serving.job_from_request(wire.decode_request(m), server.geometries) for m, _ in reqs]
+    server.run_trace(jobs, realtime=False)
+    for j, (_, x) in zip(jobs, reqs):
+        res = wire.decode_result(serving.result_message(j))
+        assert res["id"] == j.id
+        j.data = x
+        ref = alone(j, server.geometries, cuda).cpu()
+        got = torch.from_numpy(np.array(res["data"]))
+        if res["dtype"] == "bf16":
+            got = got.view(torch.int16).view(torch.bfloat16)
+        assert torch.equal(got, ref), (j.id, j.cls)
+    with pytest.raises(ValueError):  # wrong input shape for the geometry
+        serving.job_from_request(wire.decode_request(wire.encode_request(
+            9, "cone_fwd", "cone-a", "fp32", np.zeros((3, 3, 3), np.float32))), server.geometries)
