@@ -118,12 +118,20 @@ struct Cell2<__half> {
 template <typename T>
 struct CellSampler2 {
     const typename Cell2<T>::type *origin;
-    int s_x, s_y;
+    unsigned s_x, s_y;
+    unsigned bias;  // -FLOOR_BIAS * (s_x + s_y), modulo 2^32: the floors' bias folded into one offset
+
+    __device__ CellSampler2(const typename Cell2<T>::type *o, int sx, int sy)
+        : origin(o), s_x((unsigned)sx), s_y((unsigned)sy), bias(0u - (unsigned)FLOOR_BIAS * ((unsigned)sx + (unsigned)sy))
+    {
+    }
+
     __device__ __forceinline__ float operator()(float x, float y) const
     {
         const FloorFrac fx = floor_frac(x), fy = floor_frac(y);
         float v[4];
-        Cell2<T>::load(origin + (fx.i * s_x + fy.i * s_y), v);
+        const unsigned idx = (unsigned)fx.bits * s_x + (unsigned)fy.bits * s_y + bias;
+        Cell2<T>::load(origin + (int)idx, v);
         return lerp_ref(lerp_ref(v[0], v[1], fx.f), lerp_ref(v[2], v[3], fx.f), fy.f);
     }
 };
@@ -279,8 +287,8 @@ __global__ void __launch_bounds__(FP2_BLOCK)
             // rays run mostly along x (fan: the central ray)
             const bool fast_y = fabsf(ray_in.x) > fabsf(ray_in.y);
             const size_t slice = (size_t)(X + 3) * (Y + 3);
-            const CellSampler2<T> cs = fast_y ? CellSampler2<T>{cells_y + b * slice + 2 * (Y + 3) + 2, Y + 3, 1}
-                                              : CellSampler2<T>{cells_x + b * slice + 2 * (X + 3) + 2, 1, X + 3};
+            const CellSampler2<T> cs = fast_y ? CellSampler2<T>(cells_y + b * slice + 2 * (Y + 3) + 2, Y + 3, 1)
+                                              : CellSampler2<T>(cells_x + b * slice + 2 * (X + 3) + 2, 1, X + 3);
             // every position of the march lies between its two end points
             const float x0 = fmaf(a, gx, bx), y0 = fmaf(a, gy, by), x1 = fmaf(am, gx, bx), y1 = fmaf(am, gy, by);
             const float xmax = (float)X + 0.5f, ymax = (float)Y + 0.5f;
