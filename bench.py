@@ -563,7 +563,7 @@ def run_serving(args):
     with ClockSampler(physical_gpu_index(dev.index or 0)) as clk:
         s_srv = server.run_trace(jobs, realtime=True)
     jobs_plain = serving.make_jobs(trace, geos, seed=1)
-    s_plain = serving.run_plain(jobs_plain, geos, device=dev, realtime=True)
+    s_plain = serving.run_plain(jobs_plain, geos, device=dev, realtime=True, keep_results=False)
     line = {
         "metric": METRIC, "value": s_srv.gups, "unit": "GUPS", "n_gpus": 1, "steps": args.requests, "warmup": 1,
         "ms_per_step": s_srv.wall_s * 1e3 / max(1, args.requests), "higher_is_better": True, "scaling": "weak",

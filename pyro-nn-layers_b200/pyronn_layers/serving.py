@@ -15,7 +15,11 @@ geometry, FP32/BF16/FP16 storage) arrives over time.  The server
   warmed up; results stay on the device;
 * spreads batches over several CUDA streams so they overlap on the device,
   and retires each batch when its completion event has fired, admitting
-  newly arrived jobs as soon as slots and memory free up.
+  newly arrived jobs as soon as slots and memory free up;
+* runs short job classes on high-priority streams: a large job's kernel
+  fills every SM, and without priorities a short job launched beside it
+  waits until the large kernel's blocks have all started; with them the
+  block scheduler starts the short job's blocks first.
 
 Latency of a job = completion seen by the host - arrival.  ``run_trace``
 returns per-job latencies, p50/p99 and aggregate GUPS (updates: voxels x views
@@ -76,11 +80,21 @@ class ServeStats:
     batches: int
     mean_batch: float
     graph_replays: int
+    per_class: dict = dataclasses.field(default_factory=dict)  # "geometry/op" -> {n, p50_ms, p99_ms}
 
     def as_dict(self):
         return {"p50_ms": self.p50_ms, "p99_ms": self.p99_ms, "gups": self.gups, "wall_s": self.wall_s,
                 "batches": self.batches, "mean_batch": self.mean_batch, "graph_replays": self.graph_replays,
-                "jobs": int(self.latencies_ms.size)}
+                "jobs": int(self.latencies_ms.size), "per_class": self.per_class}
+
+
+def per_class_latency(jobs) -> dict:
+    """p50 / p99 latency (ms) per geometry and op (dtypes pooled)."""
+    groups = collections.defaultdict(list)
+    for j in jobs:
+        groups["%s/%s" % (j.cls.geometry, j.cls.op)].append((j.done - j.arrival) * 1e3)
+    return {k: {"n": len(v), "p50_ms": percentile(v, 50), "p99_ms": percentile(v, 99)}
+            for k, v in sorted(groups.items())}
 
 
 def percentile(values, q):
@@ -321,10 +335,16 @@ class ProjectorServer:
         self.max_inflight = max_inflight
         self.max_batch = max_batch
         self.streams = [torch.cuda.Stream(self.device) for _ in range(n_streams)]
+        # high-priority streams for short classes (lower number = higher priority)
+        _, hi = torch.cuda.Stream.priority_range() if hasattr(torch.cuda.Stream, "priority_range") else (0, -1)
+        self.fast_streams = [torch.cuda.Stream(self.device, priority=hi) for _ in range(max(1, n_streams // 2))]
+        largest = max((e.updates for e in geometries.values()), default=1)
+        self.short_updates = largest // 8  # classes at most this large are short
         self.hbm_reserve = hbm_reserve  # HBM always left free
         self.use_graphs = use_graphs
         self.keep_results = keep_results
         self.evictions = 0
+        self._budget = 0  # bytes known free above the reserve (refreshed from the device when short)
         self.clock = clock
         self.executors: Dict[JobClass, Executor] = {}
         self.batches = 0
@@ -339,6 +359,7 @@ class ProjectorServer:
         kind, geo = wire.geometry_from_descriptor(descriptor)
         entry = GeometryEntry(kind, geo, geo.volume_shape, geo.detector_shape)
         self.geometries[name] = entry
+        self.short_updates = max(e.updates for e in self.geometries.values()) // 8
         return entry
 
     def executor(self, cls: JobClass) -> Executor:
@@ -372,10 +393,19 @@ class ProjectorServer:
         """Memory admission: the batch's result copies, and the buffer set if
         it is not resident yet, must fit the free HBM above the reserve;
         idle buffer sets of other classes are evicted (oldest first) to make
-        room."""
+        room.  The device is asked for its free memory only when the budget
+        left from the last answer cannot cover the request: the query
+        (cudaMemGetInfo) can take tens of milliseconds, and asked for every
+        batch it stalled the whole loop."""
         need = (ex.result_bytes(batch) if self.keep_results else 0) + (0 if ex.allocated(bset) else ex.set_bytes())
+        if need == 0:
+            return True
+        if self._budget >= need:
+            self._budget -= need
+            return True
         free = self.free_hbm() - self.hbm_reserve
         if free >= need:
+            self._budget = free - need
             return True
         idle = sorted(((e.last_use[i], e, i) for e in self.executors.values() if e is not ex
                        for i in range(e.n_sets) if e.allocated(i) and not e.busy[i]), key=lambda r: r[0])
@@ -383,7 +413,9 @@ class ProjectorServer:
             free += e.evict(i)
             self.evictions += 1
             if free >= need:
+                self._budget = free - need
                 return True
+        self._budget = free
         return False
 
     def run_trace(self, jobs: List[Job], realtime: bool = True) -> ServeStats:
@@ -439,7 +471,9 @@ class ProjectorServer:
                 bjobs = [q.popleft() for _ in range(b)]
                 if not q:
                     del ready[cls]
-                stream = self.streams[stream_i % len(self.streams)]
+                short = self.geometries[cls.geometry].updates <= self.short_updates
+                pool = self.fast_streams if short else self.streams
+                stream = pool[stream_i % len(pool)]
                 stream_i += 1
                 inp, out, _ = ex.allocate(bset)
                 ex.busy[bset] = True
@@ -469,13 +503,16 @@ class ProjectorServer:
         lat = np.array([(j.done - j.arrival) * 1e3 for j in jobs])
         replays = sum(ex.graph_replays for ex in self.executors.values())
         return ServeStats(lat, percentile(lat, 50), percentile(lat, 99), total_updates / wall / 1e9, wall,
-                          self.batches, float(np.mean(self.batch_sizes)) if self.batch_sizes else 0.0, replays)
+                          self.batches, float(np.mean(self.batch_sizes)) if self.batch_sizes else 0.0, replays,
+                          per_class_latency(jobs))
 
 
 def run_plain(jobs: List[Job], geometries: Dict[str, GeometryEntry], device=None,
-              clock: Callable[[], float] = time.perf_counter, realtime: bool = True) -> ServeStats:
+              clock: Callable[[], float] = time.perf_counter, realtime: bool = True,
+              keep_results: bool = True) -> ServeStats:
     """The plain path: one job per launch, FP32, one stream, in arrival order,
-    each job through the public op API."""
+    each job through the public op API (results kept on the device, or
+    dropped after completion like the server's with keep_results=False)."""
     import torch
 
     from . import ops
@@ -498,14 +535,15 @@ def run_plain(jobs: List[Job], geometries: Dict[str, GeometryEntry], device=None
             r = ops.cone_projection3d(x, g.detector_shape, *g.args())
         else:
             r = ops.cone_backprojection3d(x, g.volume_shape, *g.args())
-        j.result = r[0]
+        j.result = r[0] if keep_results else None
         torch.cuda.current_stream(dev).synchronize()
         j.done = clock() - t0
         total += j.updates
     torch.cuda.synchronize(dev)
     wall = clock() - t0
     lat = np.array([(j.done - j.arrival) * 1e3 for j in jobs])
-    return ServeStats(lat, percentile(lat, 50), percentile(lat, 99), total / wall / 1e9, wall, len(jobs), 1.0, 0)
+    return ServeStats(lat, percentile(lat, 50), percentile(lat, 99), total / wall / 1e9, wall, len(jobs), 1.0, 0,
+                      per_class_latency(jobs))
 
 
 def job_from_request(req: dict, geometries: Dict[str, GeometryEntry], arrival: float = 0.0) -> Job:
