@@ -61,6 +61,46 @@ __device__ __forceinline__ float lerp_ref(float a, float b, float t)
     return __fmaf_rn(b, t, __fmaf_rn(a, -t, a));
 }
 
+// f32(h) - c for the 16-bit value h in the low (HI = false) or high half of
+// w: one mixed-precision instruction (PTX sub.f32.f16 / sub.f32.bf16, sm_100)
+// in place of a widening conversion and an FP32 subtraction (same result
+// up to FP32 subnormals, which this form does not flush).
+template <bool HI>
+__device__ __forceinline__ float sub_f32_f16(unsigned w, float c)
+{
+    float d;
+    if (HI)
+        asm("{.reg .b16 lo, hi; mov.b32 {lo, hi}, %1; sub.f32.f16 %0, hi, %2;}" : "=f"(d) : "r"(w), "f"(c));
+    else
+        asm("{.reg .b16 lo, hi; mov.b32 {lo, hi}, %1; sub.f32.f16 %0, lo, %2;}" : "=f"(d) : "r"(w), "f"(c));
+    return d;
+}
+template <bool HI>
+__device__ __forceinline__ float sub_f32_bf16(unsigned w, float c)
+{
+    float d;
+    if (HI)
+        asm("{.reg .b16 lo, hi; mov.b32 {lo, hi}, %1; sub.f32.bf16 %0, hi, %2;}" : "=f"(d) : "r"(w), "f"(c));
+    else
+        asm("{.reg .b16 lo, hi; mov.b32 {lo, hi}, %1; sub.f32.bf16 %0, lo, %2;}" : "=f"(d) : "r"(w), "f"(c));
+    return d;
+}
+
+// The first-axis lerp of a storage type's taps, on values already widened to
+// FP32: the reference's form for FP32 storage, a + t (b - a) for 16-bit
+// storage -- the form the cell samplers compute with one mixed-precision
+// subtraction, so every path of an op gives the same bits.
+template <typename T>
+__device__ __forceinline__ float lerp_first(float a, float b, float t)
+{
+    return fmaf(t, b - a, a);
+}
+template <>
+__device__ __forceinline__ float lerp_first<float>(float a, float b, float t)
+{
+    return lerp_ref(a, b, t);
+}
+
 template <typename T>
 struct type_tag {
     using type = T;

@@ -47,8 +47,8 @@ __device__ __forceinline__ float interp2d_quirk(const T *__restrict__ sino, floa
     const float p01 = (vx1 && vy0 && i01 < total) ? load_as_float(sino + i01) : 0.0f;
     const float p10 = (vx0 && vy1 && i10 < total) ? load_as_float(sino + i10) : 0.0f;
     const float p11 = (vx1 && vy1 && i11 < total) ? load_as_float(sino + i11) : 0.0f;
-    const float p0 = lerp_ref(p00, p01, tx);
-    const float p1 = lerp_ref(p10, p11, tx);
+    const float p0 = lerp_first<T>(p00, p01, tx);
+    const float p1 = lerp_first<T>(p10, p11, tx);
     return lerp_ref(p0, p1, ty);
 }
 

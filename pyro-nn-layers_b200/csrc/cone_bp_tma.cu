@@ -54,22 +54,27 @@ struct ViewMeta {
     int pad[2];
 };
 
+// lerp along u of the taps p[0], p[1] in shared memory: the reference's form
+// for FP32; for 16-bit taps a + t (b - a) with b - a one mixed-precision
+// subtraction (no widening of b)
 template <typename T>
-__device__ __forceinline__ float smem_to_float(const T *p);
+__device__ __forceinline__ float smem_ulerp(const T *p, float t);
 template <>
-__device__ __forceinline__ float smem_to_float<float>(const float *p)
+__device__ __forceinline__ float smem_ulerp<float>(const float *p, float t)
 {
-    return *p;
+    return lerp_ref(p[0], p[1], t);
 }
 template <>
-__device__ __forceinline__ float smem_to_float<__nv_bfloat16>(const __nv_bfloat16 *p)
+__device__ __forceinline__ float smem_ulerp<__half>(const __half *p, float t)
 {
-    return __bfloat162float(*p);
+    const float a = __half2float(p[0]);
+    return fmaf(t, sub_f32_f16<false>(__half_as_ushort(p[1]), a), a);
 }
 template <>
-__device__ __forceinline__ float smem_to_float<__half>(const __half *p)
+__device__ __forceinline__ float smem_ulerp<__nv_bfloat16>(const __nv_bfloat16 *p, float t)
 {
-    return __half2float(*p);
+    const float a = __bfloat162float(p[0]);
+    return fmaf(t, sub_f32_bf16<false>(__bfloat16_as_ushort(p[1]), a), a);
 }
 
 // tap rules of interp2D, cone_backprojector_3D_CudaKernel.cu.cc:55-82
@@ -91,7 +96,7 @@ __device__ __forceinline__ float interp_global(const T *__restrict__ sino, float
     const float p01 = (vx1 && vy0 && i01 < total) ? load_as_float(sino + i01) : 0.0f;
     const float p10 = (vx0 && vy1 && i10 < total) ? load_as_float(sino + i10) : 0.0f;
     const float p11 = (vx1 && vy1 && i11 < total) ? load_as_float(sino + i11) : 0.0f;
-    return lerp_ref(lerp_ref(p00, p01, tx), lerp_ref(p10, p11, tx), ty);
+    return lerp_ref(lerp_first<T>(p00, p01, tx), lerp_first<T>(p10, p11, tx), ty);
 }
 
 template <typename T>
@@ -260,11 +265,7 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
                     const FloorFrac fv = floor_frac(lv);
                     unsigned idx = (unsigned)fv.bits * (unsigned)BOX_W + col;
                     idx = min(idx, MAX_IDX);  // memory safety only: the margin keeps idx in range
-                    const float p00 = smem_to_float(tile + idx);
-                    const float p01 = smem_to_float(tile + idx + 1);
-                    const float p10 = smem_to_float(tile + idx + BOX_W);
-                    const float p11 = smem_to_float(tile + idx + BOX_W + 1);
-                    const float val = lerp_ref(lerp_ref(p00, p01, tx), lerp_ref(p10, p11, tx), fv.f);
+                    const float val = lerp_ref(smem_ulerp(tile + idx, tx), smem_ulerp(tile + idx + BOX_W, tx), fv.f);
                     acc[z] = fmaf(val, rw2, acc[z]);
                 }
             } else if (mode == MODE_SMEM) {
@@ -281,11 +282,7 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
                     const float tx = fu.f, ty = fv.f;
                     unsigned idx = (unsigned)(fv.i * BOX_W + fu.i);
                     idx = min(idx, MAX_IDX);  // memory safety only: the margin keeps idx in range
-                    const float p00 = smem_to_float(tile + idx);
-                    const float p01 = smem_to_float(tile + idx + 1);
-                    const float p10 = smem_to_float(tile + idx + BOX_W);
-                    const float p11 = smem_to_float(tile + idx + BOX_W + 1);
-                    const float val = lerp_ref(lerp_ref(p00, p01, tx), lerp_ref(p10, p11, tx), ty);
+                    const float val = lerp_ref(smem_ulerp(tile + idx, tx), smem_ulerp(tile + idx + BOX_W, tx), ty);
                     acc[z] = fmaf(val * rw, rw, acc[z]);
                 }
             } else {

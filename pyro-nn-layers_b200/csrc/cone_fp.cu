@@ -51,10 +51,10 @@ __device__ __forceinline__ float interp3d_sw(const T *__restrict__ vol, float x,
     const float p101 = (vz1 && vy0 && vx1) ? load_as_float(vol + base + sz + 1) : 0.0f;
     const float p110 = (vz1 && vy1 && vx0) ? load_as_float(vol + base + sz + sy) : 0.0f;
     const float p111 = (vz1 && vy1 && vx1) ? load_as_float(vol + base + sz + sy + 1) : 0.0f;
-    const float p00 = lerp_ref(p000, p100, tz);
-    const float p01 = lerp_ref(p001, p101, tz);
-    const float p10 = lerp_ref(p010, p110, tz);
-    const float p11 = lerp_ref(p011, p111, tz);
+    const float p00 = lerp_first<T>(p000, p100, tz);
+    const float p01 = lerp_first<T>(p001, p101, tz);
+    const float p10 = lerp_first<T>(p010, p110, tz);
+    const float p11 = lerp_first<T>(p011, p111, tz);
     const float p0 = lerp_ref(p00, p10, ty);
     const float p1 = lerp_ref(p01, p11, ty);
     return lerp_ref(p0, p1, tx);

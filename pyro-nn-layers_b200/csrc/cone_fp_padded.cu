@@ -59,6 +59,14 @@ struct Cell<float> {
         const float4 a = __ldg(&c->y0), b = __ldg(&c->y1);
         v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
     }
+    // the four z lerps of a cell: z[0] = (x0 y0), z[1] = (x1 y0), z[2] = (x0 y1), z[3] = (x1 y1)
+    __device__ static void zlerp(const CellF32 *c, float t, float (&z)[4])
+    {
+        float v[8];
+        load(c, v);
+        z[0] = lerp_ref(v[0], v[2], t), z[1] = lerp_ref(v[1], v[3], t);
+        z[2] = lerp_ref(v[4], v[6], t), z[3] = lerp_ref(v[5], v[7], t);
+    }
     __device__ static CellF32 make(const float (&v)[8])
     {
         CellF32 c;
@@ -70,15 +78,15 @@ struct Cell<float> {
 template <>
 struct Cell<__nv_bfloat16> {
     using type = uint4;
-    __device__ static void load(const uint4 *c, float (&v)[8])
+    // z lerps as a + t (b - a): the z0 tap a widened, b - a in one
+    // mixed-precision subtraction (sm_100 sub.f32.bf16), the FMA in FP32
+    __device__ static void zlerp(const uint4 *c, float t, float (&z)[4])
     {
         const uint4 w = __ldg(c);
-        const unsigned ws[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            v[2 * k] = __uint_as_float(ws[k] << 16);
-            v[2 * k + 1] = __uint_as_float(ws[k] & 0xFFFF0000u);
-        }
+        const float a0 = __uint_as_float(w.x << 16), a1 = __uint_as_float(w.x & 0xFFFF0000u);
+        const float a2 = __uint_as_float(w.z << 16), a3 = __uint_as_float(w.z & 0xFFFF0000u);
+        z[0] = fmaf(t, sub_f32_bf16<false>(w.y, a0), a0), z[1] = fmaf(t, sub_f32_bf16<true>(w.y, a1), a1);
+        z[2] = fmaf(t, sub_f32_bf16<false>(w.w, a2), a2), z[3] = fmaf(t, sub_f32_bf16<true>(w.w, a3), a3);
     }
     __device__ static uint4 make(const __nv_bfloat16 (&v)[8])
     {
@@ -92,15 +100,17 @@ struct Cell<__nv_bfloat16> {
 template <>
 struct Cell<__half> {
     using type = uint4;
-    __device__ static void load(const uint4 *c, float (&v)[8])
+    // z lerps as a + t (b - a): the z0 tap a widened, b - a in one
+    // mixed-precision subtraction (sm_100 sub.f32.f16), the FMA in FP32
+    __device__ static void zlerp(const uint4 *c, float t, float (&z)[4])
     {
         const uint4 w = __ldg(c);
-        const unsigned ws[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            v[2 * k] = __half2float(__ushort_as_half((unsigned short)(ws[k] & 0xFFFFu)));
-            v[2 * k + 1] = __half2float(__ushort_as_half((unsigned short)(ws[k] >> 16)));
-        }
+        const float a0 = __half2float(__ushort_as_half((unsigned short)(w.x & 0xFFFFu)));
+        const float a1 = __half2float(__ushort_as_half((unsigned short)(w.x >> 16)));
+        const float a2 = __half2float(__ushort_as_half((unsigned short)(w.z & 0xFFFFu)));
+        const float a3 = __half2float(__ushort_as_half((unsigned short)(w.z >> 16)));
+        z[0] = fmaf(t, sub_f32_f16<false>(w.y, a0), a0), z[1] = fmaf(t, sub_f32_f16<true>(w.y, a1), a1);
+        z[2] = fmaf(t, sub_f32_f16<false>(w.w, a2), a2), z[3] = fmaf(t, sub_f32_f16<true>(w.w, a3), a3);
     }
     __device__ static uint4 make(const __half (&v)[8])
     {
@@ -200,8 +210,8 @@ struct PaddedSampler {
         const float p100 = load_as_float(q), q_f = load_as_float(q + 1);
         const float q0s = load_as_float(q + s_row), q_fs = load_as_float(q + s_row + 1);
         // the reference's order: lerp in z, then y, then x
-        const float c00 = lerp_ref(p000, p100, fz.f), c_f = lerp_ref(p_f, q_f, fz.f);
-        const float c_s = lerp_ref(p0s, q0s, fz.f), c_fs = lerp_ref(p_fs, q_fs, fz.f);
+        const float c00 = lerp_first<T>(p000, p100, fz.f), c_f = lerp_first<T>(p_f, q_f, fz.f);
+        const float c_s = lerp_first<T>(p0s, q0s, fz.f), c_fs = lerp_first<T>(p_fs, q_fs, fz.f);
         if (FASTY) {  // fast = y, slow = x
             const float x0 = lerp_ref(c00, c_f, fy.f), x1 = lerp_ref(c_s, c_fs, fy.f);
             return lerp_ref(x0, x1, fx.f);
@@ -256,12 +266,10 @@ struct CellSampler {
     {
         const FloorFrac fx = floor_frac(x), fy = floor_frac(y), fz = floor_frac(z);
         const unsigned idx = (unsigned)fx.bits * s_x + (unsigned)fy.bits * s_y + (unsigned)fz.bits + bias;
-        float v[8];
-        Cell<T>::load(origin + (int)idx, v);
         // the reference's order: lerp in z, then y, then x
-        const float z00 = lerp_ref(v[0], v[2], fz.f), z10 = lerp_ref(v[1], v[3], fz.f);
-        const float z01 = lerp_ref(v[4], v[6], fz.f), z11 = lerp_ref(v[5], v[7], fz.f);
-        return lerp_ref(lerp_ref(z00, z01, fy.f), lerp_ref(z10, z11, fy.f), fx.f);
+        float zl[4];
+        Cell<T>::zlerp(origin + (int)idx, fz.f, zl);
+        return lerp_ref(lerp_ref(zl[0], zl[2], fy.f), lerp_ref(zl[1], zl[3], fy.f), fx.f);
     }
 };
 
@@ -281,8 +289,9 @@ struct ClampedCellSampler {
 // block's 8 x 32 results go through shared memory so the sinogram rows are
 // written 8 pixels at a time; xy mode: a warp is 32 consecutive u.
 template <typename T, typename Tout>
-// (at least 3 blocks per SM: room for the 4-sample loop's registers)
-__global__ void __launch_bounds__(PB_X *PB_Y, 3)
+// (4 blocks per SM: 64 registers hold the 4-sample loop without spills, and
+// 32 resident warps hide the cell loads better than 24 with 80 registers)
+__global__ void __launch_bounds__(PB_X *PB_Y, 4)
     cone_fp_padded_kernel(const T *__restrict__ xfast, const T *__restrict__ yfast,
                           const typename Cell<T>::type *__restrict__ cells, Tout *__restrict__ sino,
                           const ConeFpView *__restrict__ views, const float *__restrict__ step_ptr,

@@ -218,12 +218,14 @@ __device__ __forceinline__ float march_counted_x2(const ConeRay &ray, int n, flo
 
 // march_counted_x2 with four samples per iteration (their four cell loads in
 // flight together): the same samples, alpha sequence and order of additions.
+// The last sample's value is kept for the end correction instead of being
+// interpolated again (same position, same value).
 template <typename F>
 __device__ __forceinline__ float march_counted_x4(const ConeRay &ray, int n, float step, const F &sample)
 {
     float a = ray.a;
-    float px = fmaf(a, ray.dx, ray.ox), py = fmaf(a, ray.dy, ray.oy), pz = fmaf(a, ray.dz, ray.oz);
-    float pixel = 0.5f * sample(px, py, pz);
+    float last = sample(fmaf(a, ray.dx, ray.ox), fmaf(a, ray.dy, ray.oy), fmaf(a, ray.dz, ray.oz));
+    float pixel = 0.5f * last;
     a += step;
     int k = 1;
     for (; k + 3 < n; k += 4) {
@@ -231,34 +233,26 @@ __device__ __forceinline__ float march_counted_x4(const ConeRay &ray, int n, flo
         const float v0 = sample(fmaf(a, ray.dx, ray.ox), fmaf(a, ray.dy, ray.oy), fmaf(a, ray.dz, ray.oz));
         const float v1 = sample(fmaf(a1, ray.dx, ray.ox), fmaf(a1, ray.dy, ray.oy), fmaf(a1, ray.dz, ray.oz));
         const float v2 = sample(fmaf(a2, ray.dx, ray.ox), fmaf(a2, ray.dy, ray.oy), fmaf(a2, ray.dz, ray.oz));
-        px = fmaf(a3, ray.dx, ray.ox);
-        py = fmaf(a3, ray.dy, ray.oy);
-        pz = fmaf(a3, ray.dz, ray.oz);
-        const float v3 = sample(px, py, pz);
+        last = sample(fmaf(a3, ray.dx, ray.ox), fmaf(a3, ray.dy, ray.oy), fmaf(a3, ray.dz, ray.oz));
         pixel += v0;
         pixel += v1;
         pixel += v2;
-        pixel += v3;
+        pixel += last;
         a = a3 + step;
     }
     for (; k < n; ++k) {
-        px = fmaf(a, ray.dx, ray.ox);
-        py = fmaf(a, ray.dy, ray.oy);
-        pz = fmaf(a, ray.dz, ray.oz);
-        pixel += sample(px, py, pz);
+        last = sample(fmaf(a, ray.dx, ray.ox), fmaf(a, ray.dy, ray.oy), fmaf(a, ray.dz, ray.oz));
+        pixel += last;
         a += step;
     }
     pixel *= step;
     if (pixel > 0.0f) {
-        const float last_val = sample(px, py, pz);
-        pixel -= 0.5f * step * last_val;
+        pixel -= 0.5f * step * last;
         a -= step;
         const float last_step = ray.am - a;
-        pixel += 0.5f * last_step * last_val;
-        px = fmaf(ray.am, ray.dx, ray.ox);
-        py = fmaf(ray.am, ray.dy, ray.oy);
-        pz = fmaf(ray.am, ray.dz, ray.oz);
-        pixel += 0.5f * last_step * sample(px, py, pz);
+        pixel += 0.5f * last_step * last;
+        pixel += 0.5f * last_step *
+                 sample(fmaf(ray.am, ray.dx, ray.ox), fmaf(ray.am, ray.dy, ray.oy), fmaf(ray.am, ray.dz, ray.oz));
     }
     return pixel * ray.mm_scale;
 }

@@ -53,8 +53,8 @@ __device__ __forceinline__ float interp2d_border(const T *__restrict__ img, floa
     const float p01 = (vy0 && vx1) ? load_as_float(img + base + 1) : 0.0f;
     const float p10 = (vy1 && vx0) ? load_as_float(img + base + X) : 0.0f;
     const float p11 = (vy1 && vx1) ? load_as_float(img + base + X + 1) : 0.0f;
-    const float p0 = lerp_ref(p00, p01, tx);
-    const float p1 = lerp_ref(p10, p11, tx);
+    const float p0 = lerp_first<T>(p00, p01, tx);
+    const float p1 = lerp_first<T>(p10, p11, tx);
     return lerp_ref(p0, p1, ty);
 }
 
@@ -73,21 +73,23 @@ struct Cell2;
 template <>
 struct Cell2<float> {
     using type = float4;
-    __device__ static void load(const float4 *c, float (&v)[4])
+    // the two x lerps of a cell: along y0 and along y1
+    __device__ static void xlerp(const float4 *c, float t, float &x0, float &x1)
     {
         const float4 w = __ldg(c);
-        v[0] = w.x, v[1] = w.y, v[2] = w.z, v[3] = w.w;
+        x0 = lerp_ref(w.x, w.y, t), x1 = lerp_ref(w.z, w.w, t);
     }
     __device__ static float4 make(float a, float b, float c, float d) { return make_float4(a, b, c, d); }
 };
 template <>
 struct Cell2<__nv_bfloat16> {
     using type = uint2;
-    __device__ static void load(const uint2 *c, float (&v)[4])
+    // x lerps as a + t (b - a), b - a one mixed-precision subtraction
+    __device__ static void xlerp(const uint2 *c, float t, float &x0, float &x1)
     {
         const uint2 w = __ldg(c);
-        v[0] = __uint_as_float(w.x << 16), v[1] = __uint_as_float(w.x & 0xFFFF0000u);
-        v[2] = __uint_as_float(w.y << 16), v[3] = __uint_as_float(w.y & 0xFFFF0000u);
+        const float a0 = __uint_as_float(w.x << 16), a1 = __uint_as_float(w.y << 16);
+        x0 = fmaf(t, sub_f32_bf16<true>(w.x, a0), a0), x1 = fmaf(t, sub_f32_bf16<true>(w.y, a1), a1);
     }
     __device__ static uint2 make(__nv_bfloat16 a, __nv_bfloat16 b, __nv_bfloat16 c, __nv_bfloat16 d)
     {
@@ -98,13 +100,13 @@ struct Cell2<__nv_bfloat16> {
 template <>
 struct Cell2<__half> {
     using type = uint2;
-    __device__ static void load(const uint2 *c, float (&v)[4])
+    // x lerps as a + t (b - a), b - a one mixed-precision subtraction
+    __device__ static void xlerp(const uint2 *c, float t, float &x0, float &x1)
     {
         const uint2 w = __ldg(c);
-        v[0] = __half2float(__ushort_as_half((unsigned short)(w.x & 0xFFFFu)));
-        v[1] = __half2float(__ushort_as_half((unsigned short)(w.x >> 16)));
-        v[2] = __half2float(__ushort_as_half((unsigned short)(w.y & 0xFFFFu)));
-        v[3] = __half2float(__ushort_as_half((unsigned short)(w.y >> 16)));
+        const float a0 = __half2float(__ushort_as_half((unsigned short)(w.x & 0xFFFFu)));
+        const float a1 = __half2float(__ushort_as_half((unsigned short)(w.y & 0xFFFFu)));
+        x0 = fmaf(t, sub_f32_f16<true>(w.x, a0), a0), x1 = fmaf(t, sub_f32_f16<true>(w.y, a1), a1);
     }
     __device__ static uint2 make(__half a, __half b, __half c, __half d)
     {
@@ -129,10 +131,10 @@ struct CellSampler2 {
     __device__ __forceinline__ float operator()(float x, float y) const
     {
         const FloorFrac fx = floor_frac(x), fy = floor_frac(y);
-        float v[4];
         const unsigned idx = (unsigned)fx.bits * s_x + (unsigned)fy.bits * s_y + bias;
-        Cell2<T>::load(origin + (int)idx, v);
-        return lerp_ref(lerp_ref(v[0], v[1], fx.f), lerp_ref(v[2], v[3], fx.f), fy.f);
+        float x0, x1;
+        Cell2<T>::xlerp(origin + (int)idx, fx.f, x0, x1);
+        return lerp_ref(x0, x1, fy.f);
     }
 };
 
@@ -354,7 +356,7 @@ __global__ void __launch_bounds__(BP2_BLOCK_X *BP2_BLOCK_Y)
         const T *row = sino_b + (size_t)n * W;
         const float p0 = (unsigned)x0 < (unsigned)W ? load_as_float(row + x0) : 0.0f;
         const float p1 = (unsigned)(x0 + 1) < (unsigned)W ? load_as_float(row + x0 + 1) : 0.0f;
-        acc = fmaf(lerp_ref(p0, p1, t), w, acc);
+        acc = fmaf(lerp_first<T>(p0, p1, t), w, acc);
     }
     float out;
     if (!FAN)
