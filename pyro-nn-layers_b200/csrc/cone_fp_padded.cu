@@ -289,7 +289,7 @@ struct ClampedCellSampler {
 // block's 8 x 32 results go through shared memory so the sinogram rows are
 // written 8 pixels at a time; xy mode: a warp is 32 consecutive u.
 template <typename T, typename Tout>
-// (4 blocks per SM: 64 registers hold the 4-sample loop without spills, and
+// (4 blocks per SM: 64 registers hold the counted loop without spills, and
 // 32 resident warps hide the cell loads better than 24 with 80 registers)
 __global__ void __launch_bounds__(PB_X *PB_Y, 4)
     cone_fp_padded_kernel(const T *__restrict__ xfast, const T *__restrict__ yfast,
@@ -325,7 +325,9 @@ __global__ void __launch_bounds__(PB_X *PB_Y, 4)
             const int Yc = Y + 2, Zc = Z + 2;
             const CellSampler<T> s(cells + (Yc + 1) * Zc + 1, Zc, Yc * Zc);
             const int n = inside ? exact_sample_count(ray, step) : -1;
-            pixel = n > 0    ? march_counted_x4(ray, n, step, s)
+            // eight samples per iteration for 16-bit cells, four for the
+            // 32-byte FP32 cells (whose loads need twice the registers)
+            pixel = n > 0    ? march_counted<sizeof(T) == 4 ? 4 : 8>(ray, n, step, s)
                     : inside ? march_x2(ray, step, s)
                              : march_x2(ray, step, ClampedCellSampler<T>{s, xmax, ymax, zmax});
         } else {

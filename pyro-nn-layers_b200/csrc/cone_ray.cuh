@@ -216,29 +216,28 @@ __device__ __forceinline__ float march_counted_x2(const ConeRay &ray, int n, flo
     return pixel * ray.mm_scale;
 }
 
-// march_counted_x2 with four samples per iteration (their four cell loads in
+// march_counted_x2 with U samples per iteration (their U cell loads in
 // flight together): the same samples, alpha sequence and order of additions.
 // The last sample's value is kept for the end correction instead of being
 // interpolated again (same position, same value).
-template <typename F>
-__device__ __forceinline__ float march_counted_x4(const ConeRay &ray, int n, float step, const F &sample)
+template <int U, typename F>
+__device__ __forceinline__ float march_counted(const ConeRay &ray, int n, float step, const F &sample)
 {
     float a = ray.a;
     float last = sample(fmaf(a, ray.dx, ray.ox), fmaf(a, ray.dy, ray.oy), fmaf(a, ray.dz, ray.oz));
     float pixel = 0.5f * last;
     a += step;
     int k = 1;
-    for (; k + 3 < n; k += 4) {
-        const float a1 = a + step, a2 = a1 + step, a3 = a2 + step;
-        const float v0 = sample(fmaf(a, ray.dx, ray.ox), fmaf(a, ray.dy, ray.oy), fmaf(a, ray.dz, ray.oz));
-        const float v1 = sample(fmaf(a1, ray.dx, ray.ox), fmaf(a1, ray.dy, ray.oy), fmaf(a1, ray.dz, ray.oz));
-        const float v2 = sample(fmaf(a2, ray.dx, ray.ox), fmaf(a2, ray.dy, ray.oy), fmaf(a2, ray.dz, ray.oz));
-        last = sample(fmaf(a3, ray.dx, ray.ox), fmaf(a3, ray.dy, ray.oy), fmaf(a3, ray.dz, ray.oz));
-        pixel += v0;
-        pixel += v1;
-        pixel += v2;
-        pixel += last;
-        a = a3 + step;
+    for (; k + U - 1 < n; k += U) {
+        float v[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            v[j] = sample(fmaf(a, ray.dx, ray.ox), fmaf(a, ray.dy, ray.oy), fmaf(a, ray.dz, ray.oz));
+            a += step;
+        }
+#pragma unroll
+        for (int j = 0; j < U; ++j) pixel += v[j];
+        last = v[U - 1];
     }
     for (; k < n; ++k) {
         last = sample(fmaf(a, ray.dx, ray.ox), fmaf(a, ray.dy, ray.oy), fmaf(a, ray.dz, ray.oz));
