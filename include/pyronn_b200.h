@@ -95,9 +95,11 @@ PYRONN_API int pyronn_parallel_projection2d(const void *volume, void *sinogram, 
                                  void *workspace, size_t workspace_bytes, void *stream);
 
 /* Workspace bytes of a 2D forward projection (parallel or fan): two copies
- * of the batch as bilinear cells (the four taps of each cell together, zero
- * border), one x-fastest and one y-fastest, so that a sample is one load and
- * a warp's loads stay on few cache lines whatever the view direction.
+ * of the batch as bilinear cells (the four taps of each cell together, as
+ * FP32 for every in_dtype, zero border), one x-fastest and one y-fastest, so
+ * that a sample is one load and a warp's loads stay on few cache lines
+ * whatever the view direction: 2 * align256(batch * (vol_y+3) * (vol_x+3) * 16)
+ * bytes.
  * workspace may also be NULL: the call then reads the caller's volume with a
  * bounds test per tap (same results, slower). */
 PYRONN_API size_t pyronn_projection2d_workspace_size(int batch, int vol_y, int vol_x, int in_dtype);

@@ -237,9 +237,9 @@ int pyronn_release_cached_arrays(void)
 size_t pyronn_projection2d_workspace_size(int batch, int vol_y, int vol_x, int in_dtype)
 {
     if (batch <= 0 || vol_y <= 0 || vol_x <= 0 || !valid_dtype(in_dtype)) return 0;
-    // two copies of the batch as bilinear cells (4 taps each, zero border of
-    // two cells below and one above)
-    return 2 * align_up((size_t)batch * (vol_y + 3) * (vol_x + 3) * 4 * dtype_size(in_dtype), 256);
+    // two copies of the batch as bilinear cells (4 FP32 taps each, whatever
+    // the storage type; zero border of two cells below and one above)
+    return 2 * align_up((size_t)batch * (vol_y + 3) * (vol_x + 3) * 4 * sizeof(float), 256);
 }
 
 int pyronn_parallel_projection2d(const void *volume, void *sinogram, int in_dtype, int out_dtype, int batch, int vol_y, int vol_x,

@@ -14,9 +14,9 @@
 // and one y-fastest.  (The box starts half a millimetre below pixel 0: at
 // index -1 for 0.5 mm pixels, where rounding puts some rays' first sample a
 // hair below -1; the second border cell keeps every ray of such a view, and
-// so every lane of its warps, on the unclamped path.)  A sample
-// is then one 8-byte (16-bit storage) or 16-byte (FP32) load with no bounds
-// tests.  A warp's 32 threads are 32 neighbouring detector pixels, so at each
+// so every lane of its warps, on the unclamped path.)  The cells hold FP32
+// taps for every storage type, so a sample is one 16-byte load with no bounds
+// tests and no widening.  A warp's 32 threads are 32 neighbouring detector pixels, so at each
 // step their samples lie along the detector direction: views whose rays run
 // mostly along y read the x-fastest cells, the others the y-fastest ones, so
 // the warp's loads stay on few cache lines.  Without a workspace the taps are
@@ -53,8 +53,8 @@ __device__ __forceinline__ float interp2d_border(const T *__restrict__ img, floa
     const float p01 = (vy0 && vx1) ? load_as_float(img + base + 1) : 0.0f;
     const float p10 = (vy1 && vx0) ? load_as_float(img + base + X) : 0.0f;
     const float p11 = (vy1 && vx1) ? load_as_float(img + base + X + 1) : 0.0f;
-    const float p0 = lerp_first<T>(p00, p01, tx);
-    const float p1 = lerp_first<T>(p10, p11, tx);
+    const float p0 = lerp_ref(p00, p01, tx);
+    const float p1 = lerp_ref(p10, p11, tx);
     return lerp_ref(p0, p1, ty);
 }
 
@@ -66,13 +66,12 @@ struct BorderSampler {
 };
 
 // The four taps of a bilinear cell in the order V(x0,y0), V(x1,y0),
-// V(x0,y1), V(x1,y1): a float4 for FP32, two words of two 16-bit values for
-// BF16 / FP16 (x0 in the low half).
-template <typename T>
-struct Cell2;
-template <>
-struct Cell2<float> {
-    using type = float4;
+// V(x0,y1), V(x1,y1), widened to FP32 whatever the storage type: the
+// forward is bound by instruction issue, not by bytes (the slices' cells sit
+// in L2), and FP32 taps need no widening per sample (measured on the 64 x 512^2
+// fan batch: FP16 cells 43.7 ms, FP32 cells 42.3 ms per forward).  Widening is
+// exact, so 16-bit storage gives the FP32 result of the rounded input.
+struct Cell2 {
     // the two x lerps of a cell: along y0 and along y1
     __device__ static void xlerp(const float4 *c, float t, float &x0, float &x1)
     {
@@ -81,49 +80,15 @@ struct Cell2<float> {
     }
     __device__ static float4 make(float a, float b, float c, float d) { return make_float4(a, b, c, d); }
 };
-template <>
-struct Cell2<__nv_bfloat16> {
-    using type = uint2;
-    // x lerps as a + t (b - a), b - a one mixed-precision subtraction
-    __device__ static void xlerp(const uint2 *c, float t, float &x0, float &x1)
-    {
-        const uint2 w = __ldg(c);
-        const float a0 = __uint_as_float(w.x << 16), a1 = __uint_as_float(w.y << 16);
-        x0 = fmaf(t, sub_f32_bf16<true>(w.x, a0), a0), x1 = fmaf(t, sub_f32_bf16<true>(w.y, a1), a1);
-    }
-    __device__ static uint2 make(__nv_bfloat16 a, __nv_bfloat16 b, __nv_bfloat16 c, __nv_bfloat16 d)
-    {
-        return make_uint2((unsigned)__bfloat16_as_ushort(a) | ((unsigned)__bfloat16_as_ushort(b) << 16),
-                          (unsigned)__bfloat16_as_ushort(c) | ((unsigned)__bfloat16_as_ushort(d) << 16));
-    }
-};
-template <>
-struct Cell2<__half> {
-    using type = uint2;
-    // x lerps as a + t (b - a), b - a one mixed-precision subtraction
-    __device__ static void xlerp(const uint2 *c, float t, float &x0, float &x1)
-    {
-        const uint2 w = __ldg(c);
-        const float a0 = __half2float(__ushort_as_half((unsigned short)(w.x & 0xFFFFu)));
-        const float a1 = __half2float(__ushort_as_half((unsigned short)(w.y & 0xFFFFu)));
-        x0 = fmaf(t, sub_f32_f16<true>(w.x, a0), a0), x1 = fmaf(t, sub_f32_f16<true>(w.y, a1), a1);
-    }
-    __device__ static uint2 make(__half a, __half b, __half c, __half d)
-    {
-        return make_uint2((unsigned)__half_as_ushort(a) | ((unsigned)__half_as_ushort(b) << 16),
-                          (unsigned)__half_as_ushort(c) | ((unsigned)__half_as_ushort(d) << 16));
-    }
-};
 
 // Bilinear interpolation from a cell copy; `origin` is the cell of floor
 // (0, 0), (s_x, s_y) the cell strides.  Floors must lie in [-2, N].
-template <typename T>
 struct CellSampler2 {
-    const typename Cell2<T>::type *origin;
+    const float4 *origin;
     unsigned s_x, s_y;
     unsigned bias;  // -FLOOR_BIAS * (s_x + s_y), modulo 2^32: the floors' bias folded into one offset
 
-    __device__ CellSampler2(const typename Cell2<T>::type *o, int sx, int sy)
+    __device__ CellSampler2(const float4 *o, int sx, int sy)
         : origin(o), s_x((unsigned)sx), s_y((unsigned)sy), bias(0u - (unsigned)FLOOR_BIAS * ((unsigned)sx + (unsigned)sy))
     {
     }
@@ -133,16 +98,15 @@ struct CellSampler2 {
         const FloorFrac fx = floor_frac(x), fy = floor_frac(y);
         const unsigned idx = (unsigned)fx.bits * s_x + (unsigned)fy.bits * s_y + bias;
         float x0, x1;
-        Cell2<T>::xlerp(origin + (int)idx, fx.f, x0, x1);
+        Cell2::xlerp(origin + (int)idx, fx.f, x0, x1);
         return lerp_ref(x0, x1, fy.f);
     }
 };
 
 // For rays whose march leaves [-1.5, N + 0.5]: positions clamped into it,
 // which changes no tap weight that is not zero either way.
-template <typename T>
 struct ClampedCellSampler2 {
-    CellSampler2<T> s;
+    CellSampler2 s;
     float xmax, ymax;
     __device__ __forceinline__ float operator()(float x, float y) const
     {
@@ -223,8 +187,8 @@ __device__ __forceinline__ float march2d(float a, float am, float step, float gx
 
 template <typename T, typename Tout, bool FAN>
 __global__ void __launch_bounds__(FP2_BLOCK)
-    projection2d_kernel(const T *__restrict__ vol, const typename Cell2<T>::type *__restrict__ cells_x,
-                        const typename Cell2<T>::type *__restrict__ cells_y, Tout *__restrict__ sino, Geom2D geo,
+    projection2d_kernel(const T *__restrict__ vol, const float4 *__restrict__ cells_x,
+                        const float4 *__restrict__ cells_y, Tout *__restrict__ sino, Geom2D geo,
                         int X, int Y, int W, int n_proj, int geom_batch)
 {
     const int u = blockIdx.x * FP2_BLOCK + threadIdx.x;
@@ -289,15 +253,15 @@ __global__ void __launch_bounds__(FP2_BLOCK)
             // rays run mostly along x (fan: the central ray)
             const bool fast_y = fabsf(ray_in.x) > fabsf(ray_in.y);
             const size_t slice = (size_t)(X + 3) * (Y + 3);
-            const CellSampler2<T> cs = fast_y ? CellSampler2<T>(cells_y + b * slice + 2 * (Y + 3) + 2, Y + 3, 1)
-                                              : CellSampler2<T>(cells_x + b * slice + 2 * (X + 3) + 2, 1, X + 3);
+            const CellSampler2 cs = fast_y ? CellSampler2(cells_y + b * slice + 2 * (Y + 3) + 2, Y + 3, 1)
+                                           : CellSampler2(cells_x + b * slice + 2 * (X + 3) + 2, 1, X + 3);
             // every position of the march lies between its two end points
             const float x0 = fmaf(a, gx, bx), y0 = fmaf(a, gy, by), x1 = fmaf(am, gx, bx), y1 = fmaf(am, gy, by);
             const float xmax = (float)X + 0.5f, ymax = (float)Y + 0.5f;
             const bool inside = fminf(x0, x1) >= -1.5f && fminf(y0, y1) >= -1.5f && fmaxf(x0, x1) <= xmax &&
                                 fmaxf(y0, y1) <= ymax;
             pixel = inside ? march2d(a, am, step, gx, bx, gy, by, cs)
-                           : march2d(a, am, step, gx, bx, gy, by, ClampedCellSampler2<T>{cs, xmax, ymax});
+                           : march2d(a, am, step, gx, bx, gy, by, ClampedCellSampler2{cs, xmax, ymax});
         } else {
             pixel = march2d(a, am, step, gx, bx, gy, by, BorderSampler<T>{vol + (size_t)b * X * Y, X, Y});
         }
@@ -372,10 +336,10 @@ __global__ void __launch_bounds__(BP2_BLOCK_X *BP2_BLOCK_Y)
 // (along y); grid (ceil((X+3)/32), ceil((Y+3)/32), batch), block 32 x 8.
 template <typename T>
 __global__ void __launch_bounds__(256) pad_cells2d_kernel(const T *__restrict__ in,
-                                                          typename Cell2<T>::type *__restrict__ cells_x,
-                                                          typename Cell2<T>::type *__restrict__ cells_y, int X, int Y)
+                                                          float4 *__restrict__ cells_x,
+                                                          float4 *__restrict__ cells_y, int X, int Y)
 {
-    __shared__ T tile[33][34];  // [y - (yc0-2)][x - (xc0-2)]
+    __shared__ float tile[33][34];  // [y - (yc0-2)][x - (xc0-2)], widened
     const int Xc = X + 3, Yc = Y + 3;
     const int xc0 = blockIdx.x * 32, yc0 = blockIdx.y * 32;
     const T *img = in + (size_t)blockIdx.z * X * Y;
@@ -383,8 +347,8 @@ __global__ void __launch_bounds__(256) pad_cells2d_kernel(const T *__restrict__ 
         const int y = yc0 - 2 + r;
         for (int c = threadIdx.x; c < 33; c += 32) {
             const int x = xc0 - 2 + c;
-            T v = T(0.0f);
-            if (y >= 0 && y < Y && x >= 0 && x < X) v = img[(size_t)y * X + x];
+            float v = 0.0f;
+            if (y >= 0 && y < Y && x >= 0 && x < X) v = load_as_float(img + (size_t)y * X + x);
             tile[r][c] = v;
         }
     }
@@ -394,13 +358,13 @@ __global__ void __launch_bounds__(256) pad_cells2d_kernel(const T *__restrict__ 
         {  // x-fastest: thread x along xc
             const int xc = xc0 + threadIdx.x, yc = yc0 + r;
             if (xc < Xc && yc < Yc)
-                cells_x[slice + (size_t)yc * Xc + xc] = Cell2<T>::make(
+                cells_x[slice + (size_t)yc * Xc + xc] = Cell2::make(
                     tile[r][threadIdx.x], tile[r][threadIdx.x + 1], tile[r + 1][threadIdx.x], tile[r + 1][threadIdx.x + 1]);
         }
         {  // y-fastest: thread x along yc
             const int yc = yc0 + threadIdx.x, xc = xc0 + r;
             if (xc < Xc && yc < Yc)
-                cells_y[slice + (size_t)xc * Yc + yc] = Cell2<T>::make(
+                cells_y[slice + (size_t)xc * Yc + yc] = Cell2::make(
                     tile[threadIdx.x][r], tile[threadIdx.x][r + 1], tile[threadIdx.x + 1][r], tile[threadIdx.x + 1][r + 1]);
         }
     }
@@ -410,7 +374,7 @@ template <typename Tin, typename Tout>
 cudaError_t fp_typed(const void *volume, void *sinogram, bool fan, const Dims2D &d, const Geom2D &g,
                      void *workspace, cudaStream_t stream)
 {
-    using C = typename Cell2<Tin>::type;
+    using C = float4;
     C *cells_x = nullptr, *cells_y = nullptr;
     if (workspace) {
         const size_t n = (size_t)d.batch * (d.vol_x + 3) * (d.vol_y + 3);

@@ -91,10 +91,10 @@ def test_null_pointers_and_dims():
 
 def test_2d_forward_workspace_size_and_checks():
     lib = _capi.load()
-    # two cell copies of the batch (4 taps per cell, border of two cells
-    # below and one above), each rounded up to 256 bytes
+    # two cell copies of the batch (4 FP32 taps per cell whatever the storage
+    # type, border of two cells below and one above), each rounded up to 256 bytes
     assert _capi.workspace_size("pyronn_projection2d", 3, 5, 7, 0) == 2 * 3840
-    assert _capi.workspace_size("pyronn_projection2d", 2, 100, 100, 1) == 2 * 169984
+    assert _capi.workspace_size("pyronn_projection2d", 2, 100, 100, 1) == 2 * 339712
     assert _capi.workspace_size("pyronn_projection2d", 0, 5, 7, 0) == 0
     assert _capi.workspace_size("pyronn_projection2d", 1, 5, 7, 9) == 0
     st = lib.pyronn_fan_projection2d(FAKE, FAKE, 0, 0, 2, 10, 10, 3, 5, FAKE, FAKE, FAKE, FAKE, FAKE, FAKE, FAKE, 1,
