@@ -26,6 +26,7 @@
 // Backward (ParallelBackprojection2D / FanBackprojection2D): one thread per
 // pixel, loop over views, linear interpolation along the detector row.
 #include <math_constants.h>
+#include <type_traits>
 
 #include "common.cuh"
 #include "internal.h"
@@ -38,6 +39,7 @@ constexpr float PI_REF = 3.14159265359f;  // par_backprojector_2D_CudaKernel.cu.
 constexpr int FP2_BLOCK = 128;
 constexpr int BP2_BLOCK_X = 32;
 constexpr int BP2_BLOCK_Y = 8;
+constexpr int BP2_CHUNK = BP2_BLOCK_X * BP2_BLOCK_Y;  // views per shared-memory table
 
 template <typename T>
 __device__ __forceinline__ float interp2d_border(const T *__restrict__ img, float x, float y, int X, int Y)
@@ -115,7 +117,7 @@ struct ClampedCellSampler2 {
 };
 
 // The ray march of kernel_project2D (par_projector_2D_CudaKernel.cu.cc:58-102)
-// at positions (bx + a gx, by + a gy) in index space, four (then two, then
+// at positions (bx + a gx, by + a gy) in index space, eight (then four, two,
 // one) samples per iteration (their gathers overlap) with the same alpha
 // sequence and order of additions as one at a time.
 template <typename F>
@@ -132,6 +134,32 @@ __device__ __forceinline__ float march2d(float a, float am, float step, float gx
         pixel += 0.5f * sample(px, py);
         a += step;
         ++iter;
+    }
+    // eight samples per compare while the eighth alpha is still before the exit
+    while (iter + 7 < max_iter) {
+        const float a1 = a + step, a2 = a1 + step, a3 = a2 + step, a4 = a3 + step, a5 = a4 + step, a6 = a5 + step,
+                    a7 = a6 + step;
+        if (!(a7 < am)) break;
+        const float v0 = sample(fmaf(a, gx, bx), fmaf(a, gy, by));
+        const float v1 = sample(fmaf(a1, gx, bx), fmaf(a1, gy, by));
+        const float v2 = sample(fmaf(a2, gx, bx), fmaf(a2, gy, by));
+        const float v3 = sample(fmaf(a3, gx, bx), fmaf(a3, gy, by));
+        const float v4 = sample(fmaf(a4, gx, bx), fmaf(a4, gy, by));
+        const float v5 = sample(fmaf(a5, gx, bx), fmaf(a5, gy, by));
+        const float v6 = sample(fmaf(a6, gx, bx), fmaf(a6, gy, by));
+        px = fmaf(a7, gx, bx);
+        py = fmaf(a7, gy, by);
+        const float v7 = sample(px, py);
+        pixel += v0;
+        pixel += v1;
+        pixel += v2;
+        pixel += v3;
+        pixel += v4;
+        pixel += v5;
+        pixel += v6;
+        pixel += v7;
+        a = a7 + step;
+        iter += 8;
     }
     // four samples per compare while the fourth alpha is still before the
     // exit (the sequence never decreases, so the first three are too)
@@ -186,7 +214,9 @@ __device__ __forceinline__ float march2d(float a, float am, float step, float gx
 }
 
 template <typename T, typename Tout, bool FAN>
-__global__ void __launch_bounds__(FP2_BLOCK)
+// (12 blocks per SM: 40 registers hold the eight-sample loop; the kernel is
+// bound by the cell loads' latency, so more resident warps pay)
+__global__ void __launch_bounds__(FP2_BLOCK, 12)
     projection2d_kernel(const T *__restrict__ vol, const float4 *__restrict__ cells_x,
                         const float4 *__restrict__ cells_y, Tout *__restrict__ sino, Geom2D geo,
                         int X, int Y, int W, int n_proj, int geom_batch)
@@ -270,20 +300,56 @@ __global__ void __launch_bounds__(FP2_BLOCK)
     store_from_float(sino + ((size_t)b * n_proj + p) * W + u, pixel);
 }
 
+// Linear interpolation of a sinogram row at floor x0 with weight t, taps
+// outside [0, W) zero: the reference's form for FP32; for 16-bit storage
+// a + t (b - a) with b - a one mixed-precision subtraction (lerp_first's bits).
+template <typename T>
+struct RowTaps {
+    __device__ static __forceinline__ float lerp(const T *row, int x0, int W, float t)
+    {
+        const unsigned short r0 = (unsigned)x0 < (unsigned)W ? __ldg(reinterpret_cast<const unsigned short *>(row + x0)) : 0;
+        const unsigned short r1 =
+            (unsigned)(x0 + 1) < (unsigned)W ? __ldg(reinterpret_cast<const unsigned short *>(row + x0 + 1)) : 0;
+        if (std::is_same<T, __half>::value) {
+            const float a = __half2float(__ushort_as_half(r0));
+            return fmaf(t, sub_f32_f16<false>(r1, a), a);
+        } else {
+            const float a = __uint_as_float((unsigned)r0 << 16);
+            return fmaf(t, sub_f32_bf16<false>(r1, a), a);
+        }
+    }
+};
+template <>
+struct RowTaps<float> {
+    __device__ static __forceinline__ float lerp(const float *row, int x0, int W, float t)
+    {
+        const float p0 = (unsigned)x0 < (unsigned)W ? __ldg(row + x0) : 0.0f;
+        const float p1 = (unsigned)(x0 + 1) < (unsigned)W ? __ldg(row + x0 + 1) : 0.0f;
+        return lerp_ref(p0, p1, t);
+    }
+};
+
+// One thread per pixel, views in chunks of BP2_CHUNK whose per-view
+// constants the block first puts in shared memory (one view per thread):
+// parallel beam (-r.y, r.x) / detector spacing, fan beam (r.x, r.y, SID |r|^2,
+// SDD |r|^2 / detector spacing), so a view costs each pixel one broadcast load.
 template <typename T, typename Tout, bool FAN>
 __global__ void __launch_bounds__(BP2_BLOCK_X *BP2_BLOCK_Y)
     backprojection2d_kernel(const T *__restrict__ sino, Tout *__restrict__ vol, Geom2D geo, int X, int Y, int W,
                             int n_proj, int geom_batch)
 {
+    __shared__ float4 tab[BP2_CHUNK];
     const int i = blockIdx.x * BP2_BLOCK_X + threadIdx.x;
     const int j = blockIdx.y * BP2_BLOCK_Y + threadIdx.y;
+    const int tid = threadIdx.y * BP2_BLOCK_X + threadIdx.x;
     const int b = blockIdx.z;
-    if (i >= X || j >= Y) return;
+    const bool live = i < X && j < Y;
     const int g = geom_batch == 1 ? 0 : b;
     const float sx = geo.volume_spacing[2 * g + 1], sy = geo.volume_spacing[2 * g + 0];
     const float ox = geo.volume_origin[2 * g + 1], oy = geo.volume_origin[2 * g + 0];
     const float ds = geo.detector_spacing[g], dorg = geo.detector_origin[g];
     const float ids = 1.0f / ds;
+    const float sdo = dorg * ids;  // detector origin in pixels
     const float cx = (float)i * sx + ox, cy = (float)j * sy + oy;
     const float2 *rays = reinterpret_cast<const float2 *>(geo.rays) + (size_t)g * n_proj;
     const T *sino_b = sino + (size_t)b * n_proj * W;
@@ -293,35 +359,46 @@ __global__ void __launch_bounds__(BP2_BLOCK_X *BP2_BLOCK_Y)
         sdd = geo.sdd[g];
     }
     float acc = 0.0f;
-    for (int n = 0; n < n_proj; ++n) {
-        const float2 r = __ldg(&rays[n]);
-        // detector direction (-r.y, r.x), par_backprojector_2D_CudaKernel.cu.cc:48-49
-        float s, w = 1.0f;
-        if (!FAN) {
-            s = cx * -r.y + cy * r.x;  // :51
-        } else {
-            // intersectLines2D(pixel, source, centre, centre + det) of
-            // fan_backprojector_2D_CudaKernel.cu.cc:52-57 in closed form:
-            // s = SDD |r|^2 <c, d> / (<c, r> + SID |r|^2), weight 1 / |c - src|^2
-            const float rr = r.x * r.x + r.y * r.y;
-            const float cd = cx * -r.y + cy * r.x;
-            const float cr = cx * r.x + cy * r.y;
-            s = sdd * rr * cd * fast_rcp(fmaf(sid, rr, cr));
-            const float ex = fmaf(r.x, sid, cx), ey = fmaf(r.y, sid, cy);
-            w = fast_rcp(fmaf(ex, ex, ey * ey));
+    for (int n0 = 0; n0 < n_proj; n0 += BP2_CHUNK) {
+        const int cnt = min(BP2_CHUNK, n_proj - n0);
+        __syncthreads();  // the previous chunk's constants are no longer read
+        if (tid < cnt) {
+            const float2 r = __ldg(&rays[n0 + tid]);
+            if (FAN) {
+                const float rr = r.x * r.x + r.y * r.y;
+                tab[tid] = make_float4(r.x, r.y, sid * rr, sdd * rr * ids);
+            } else {
+                // detector direction (-r.y, r.x), par_backprojector_2D_CudaKernel.cu.cc:48-49
+                tab[tid] = make_float4(-r.y * ids, r.x * ids, 0.0f, 0.0f);
+            }
         }
-        const float sidx = (s - dorg) * ids;
-        // detector positions of pixels inside the field stay far below 2^22;
-        // a pixel whose position is larger misses the row either way
-        const float sc = fminf(fmaxf(sidx, -4.0f), (float)W + 4.0f);
-        const FloorFrac ff = floor_frac(sc);
-        const float t = ff.f;
-        const int x0 = ff.i;
-        const T *row = sino_b + (size_t)n * W;
-        const float p0 = (unsigned)x0 < (unsigned)W ? load_as_float(row + x0) : 0.0f;
-        const float p1 = (unsigned)(x0 + 1) < (unsigned)W ? load_as_float(row + x0 + 1) : 0.0f;
-        acc = fmaf(lerp_first<T>(p0, p1, t), w, acc);
+        __syncthreads();
+        if (!live) continue;
+        const T *row = sino_b + (size_t)n0 * W;
+#pragma unroll 4
+        for (int k = 0; k < cnt; ++k, row += W) {
+            const float4 q = tab[k];
+            float sidx, w = 1.0f;
+            if (!FAN) {
+                sidx = fmaf(cx, q.x, fmaf(cy, q.y, -sdo));  // (<c, d> - origin) / spacing, :51
+            } else {
+                // intersectLines2D(pixel, source, centre, centre + det) of
+                // fan_backprojector_2D_CudaKernel.cu.cc:52-57 in closed form:
+                // s = SDD |r|^2 <c, d> / (<c, r> + SID |r|^2), weight 1 / |c - src|^2
+                const float cd = fmaf(cy, q.x, -cx * q.y);
+                const float cr = fmaf(cx, q.x, cy * q.y);
+                sidx = fmaf(q.w * cd, fast_rcp(cr + q.z), -sdo);
+                const float ex = fmaf(q.x, sid, cx), ey = fmaf(q.y, sid, cy);
+                w = fast_rcp(fmaf(ex, ex, ey * ey));
+            }
+            // detector positions of pixels inside the field stay far below 2^22;
+            // a pixel whose position is larger misses the row either way
+            const float sc = fminf(fmaxf(sidx, -4.0f), (float)W + 4.0f);
+            const FloorFrac ff = floor_frac(sc);
+            acc = fmaf(RowTaps<T>::lerp(row, ff.i, W, ff.f), w, acc);
+        }
     }
+    if (!live) return;
     float out;
     if (!FAN)
         out = PI_REF * acc / (float)n_proj;  // :58
