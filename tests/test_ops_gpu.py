@@ -476,6 +476,26 @@ def test_cone_tiny_and_ragged_shapes(cuda, vol_shape, det, n_proj, batch, hw):
     assert rel_l2(back.cpu().numpy(), refb) < (5e-3 if hw else 1e-5) or np.abs(refb).max() == 0
 
 
+@pytest.mark.parametrize("n_proj", [256, 300, 513])
+@pytest.mark.parametrize("fan", [False, True])
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float16])
+def test_2d_backprojection_view_chunks(cuda, n_proj, fan, dtype):
+    """The 2D backprojector stages the views' constants in shared memory 256 at
+    a time: one full chunk, a full chunk and a ragged one, and three chunks
+    whose last holds one view, against the oracle."""
+    if fan:
+        geo = geometry.FanBeam2D((24, 20), (1.0, 0.8), 40, 1.1, n_proj, 40.0, 70.0)
+        bwd, obwd = pl.fan_backprojection2d, oracle.fan_backprojection2d
+    else:
+        geo = geometry.ParallelBeam2D((24, 20), (1.0, 0.8), 40, 1.1, n_proj)
+        bwd, obwd = pl.parallel_backprojection2d, oracle.parallel_backprojection2d
+    rng = np.random.Generator(np.random.PCG64(n_proj))
+    sino = t(rng.uniform(0.2, 1.0, (2,) + geo.detector_shape).astype(np.float32), cuda, dtype)
+    back = bwd(sino, geo.volume_shape, *geo.args(), out_dtype=torch.float32)
+    refb = obwd(rounded(sino), geo.volume_shape, *geo.args())
+    assert rel_l2(back.cpu().numpy(), refb) < 1e-5
+
+
 @pytest.mark.parametrize("vol_shape,det_w,n_proj,batch", [((1, 1), 1, 1, 1), ((5, 3), 7, 2, 3), ((2, 33), 4, 5, 1)])
 @pytest.mark.parametrize("fan", [False, True])
 def test_2d_tiny_and_ragged_shapes(cuda, vol_shape, det_w, n_proj, batch, fan):
