@@ -718,6 +718,11 @@ def run_fdk(args):
     b_ms = statistics.mean(b.elapsed_time(c) for _, b, c in ev)
     wp = (W + 15) // 16 * 16
     flops = 2.0 * n * H * wp * (wp / 2 + 1)
+    # the tensor-core filter's executed work: three TF32 products (hi*hi,
+    # hi*lo, lo*hi) of the dense Toeplitz matrix, outputs in tiles of 128,
+    # inputs in chunks of 32
+    wn, wk = (W + 127) // 128 * 128, (W + 31) // 32 * 32
+    tc_flops = 3 * 2.0 * n * H * wn * wk
     line = {
         "metric": "cone-beam FDK (filter + backprojection) GUPS", "value": updates(cfg) * args.steps / (ms / 1e3) / 1e9,
         "unit": "GUPS", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
@@ -727,8 +732,11 @@ def run_fdk(args):
                    "filter": "ram-lak", "filtered_storage": "fp32"},
         "kernels": {"filter_ms": f_ms, "backprojection_ms": b_ms,
                     "filter_tflops": flops / (f_ms / 1e3) / 1e12,
-                    "filter_note": "FP32 FMAs of the direct convolution over the nonzero Ram-Lak taps, "
-                                   "2 x rows x %d x (%d / 2 + 1) per launch" % (wp, wp)},
+                    "filter_note": "useful work: the FP32 FMAs of a direct convolution over the nonzero Ram-Lak "
+                                   "taps, 2 x rows x %d x (%d / 2 + 1) per launch" % (wp, wp),
+                    "filter_tensor_tflops": tc_flops / (f_ms / 1e3) / 1e12,
+                    "filter_tensor_note": "executed on the tensor cores (rows up to 4096 pixels): 3 TF32 "
+                                          "products x 2 x rows x %d x %d per launch" % (wn, wk)},
         "clocks": clk.summary(),
     }
     print(json.dumps(line))

@@ -20,6 +20,7 @@
 // (half the FMAs and tap loads) and adds the centre tap after.  Results are
 // staged through shared memory so the rows are written coalesced.
 #include "common.cuh"
+#include "fdk_taps.cuh"
 #include "internal.h"
 
 namespace pyronn {
@@ -64,16 +65,7 @@ __global__ void __launch_bounds__(256)
 
     // tau * h[m], in FP64, rounded once
     const int nt = tap_count(W);
-    const double pi2 = 9.869604401089358;  // pi^2
-    for (int i = tid; i < nt; i += nthreads) {
-        const double m = (double)(i - (Wp - 1));
-        double t;
-        if (kind == 0)
-            t = (m == 0.0) ? 0.25 / du : ((((long long)m) & 1) ? -1.0 / (pi2 * m * m * du) : 0.0);
-        else
-            t = -2.0 / (pi2 * du * (4.0 * m * m - 1.0));
-        taps[skew(i)] = (float)t;
-    }
+    for (int i = tid; i < nt; i += nthreads) taps[skew(i)] = fdk_tap(kind, i - (Wp - 1), du);
 
     const long long row = (long long)blockIdx.x * blockDim.y + threadIdx.y;
     const bool live = row < rows;
@@ -152,6 +144,15 @@ cudaError_t launch_fdk_filter(const void *in, void *out, int in_dtype, int out_d
                               int W, float sdd, float dv, float du, float cv, float cu, int kind, int weight_output,
                               cudaStream_t stream)
 {
+    // the tensor-core kernel reads a row's inputs from every output tile of
+    // it, so it needs distinct input and output buffers; in-place calls take
+    // the CUDA-core kernel, which holds whole rows in shared memory
+    const char *ib = (const char *)in, *ob = (const char *)out;
+    const size_t n = (size_t)rows * (size_t)W;
+    const bool overlap = ib < ob + n * dtype_size(out_dtype) && ob < ib + n * dtype_size(in_dtype);
+    if (fdk_tc_supported(rows, W, in, out) && !overlap)
+        return launch_fdk_filter_tc(in, out, in_dtype, out_dtype, rows, det_h, W, sdd, dv, du, cv, cu, kind,
+                                    weight_output, stream);
     const int chunks = (W + FB - 1) / FB;
     const int tpr = (chunks + 31) / 32 * 32;  // threads per row, a warp multiple
     const int rpb = 256 / tpr > 0 ? 256 / tpr : 1;

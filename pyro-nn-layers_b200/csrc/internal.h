@@ -70,6 +70,12 @@ cudaError_t launch_cone_fp_padded(const void *volume, void *sinogram, int in_dty
 cudaError_t launch_fdk_filter(const void *in, void *out, int in_dtype, int out_dtype, long long rows, int det_h,
                               int W, float sdd, float dv, float du, float cv, float cu, int kind, int weight_output,
                               cudaStream_t stream);
+// the same on the tensor cores (fdk_tc.cu): rows of at most 2048 pixels, a
+// multiple of 4, 16-byte aligned buffers, at most 65535 * 128 rows
+bool fdk_tc_supported(long long rows, int W, const void *in, const void *out);
+cudaError_t launch_fdk_filter_tc(const void *in, void *out, int in_dtype, int out_dtype, long long rows, int det_h,
+                                 int W, float sdd, float dv, float du, float cv, float cu, int kind,
+                                 int weight_output, cudaStream_t stream);
 
 cudaError_t launch_cone_scatter(const void *sinogram, float *volume, int in_dtype, const Dims3D &d,
                                 const ConeFpView *views, const float *step, const float *spacing,

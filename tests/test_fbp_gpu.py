@@ -52,8 +52,10 @@ def test_fdk_filter_storage_types(cuda, dtype):
 
 
 def test_fdk_filter_in_place_and_adjoint(cuda):
-    """In-place filtering equals out-of-place; the weight_output form is the
-    adjoint (dot-product test), which is also the autograd backward."""
+    """In-place filtering (the CUDA-core kernel, which holds whole rows in
+    shared memory) agrees with out-of-place filtering (the tensor-core kernel)
+    to FP32 rounding; the weight_output form is the adjoint (dot-product
+    test), which is also the autograd backward."""
     rng = np.random.Generator(np.random.PCG64(23))
     x = torch.as_tensor(rng.uniform(-1, 1, (2, 3, 5, 48)), dtype=torch.float32, device=cuda)
     y = torch.as_tensor(rng.uniform(-1, 1, (2, 3, 5, 48)), dtype=torch.float32, device=cuda)
@@ -61,7 +63,7 @@ def test_fdk_filter_in_place_and_adjoint(cuda):
     xi = x.clone()
     _capi.call("pyronn_fdk_filter", xi.data_ptr(), xi.data_ptr(), 0, 0, 2, 3, 5, 48, 700.0, 0.9, 1.2, 2.0, 23.5,
                0, 0, torch.cuda.current_stream().cuda_stream)
-    torch.testing.assert_close(xi, fx, rtol=0, atol=0)
+    assert rel_l2(xi.cpu().numpy(), fx.cpu().numpy()) < 3e-6
     xg = x.clone().requires_grad_(True)
     (fbp.fdk_filter(xg, 700.0, (0.9, 1.2)) * y).sum().backward()
     lhs = float((fx.double() * y.double()).sum())
