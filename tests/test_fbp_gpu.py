@@ -26,6 +26,9 @@ pytestmark = pytest.mark.gpu
     ((1, 3, 4, 77), 450.0, (1.3, 40.2)),   # width not a multiple of 16, offset principal point
     ((2, 6, 1, 200), 0.0, None),           # parallel-beam rows: no weighting
     ((1, 2, 3, 1030), 1200.0, None),       # wide rows: several warps per row
+    ((1, 3, 130, 1024), 1200.0, None),     # tensor cores: 8 output tiles, 4 accumulators, a partial row block
+    ((1, 1, 5, 2048), 1000.0, (2.0, 1000.5)),  # tensor cores at their widest rows (64 chunks per accumulator set)
+    ((1, 1, 2, 2052), 1000.0, None),       # just past the tensor-core width: CUDA cores
 ])
 def test_fdk_filter_vs_oracle(cuda, filt, shape, sdd, pp):
     rng = np.random.Generator(np.random.PCG64(21))
