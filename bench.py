@@ -735,7 +735,7 @@ def run_fdk(args):
                     "filter_note": "useful work: the FP32 FMAs of a direct convolution over the nonzero Ram-Lak "
                                    "taps, 2 x rows x %d x (%d / 2 + 1) per launch" % (wp, wp),
                     "filter_tensor_tflops": tc_flops / (f_ms / 1e3) / 1e12,
-                    "filter_tensor_note": "executed on the tensor cores (rows up to 4096 pixels): 3 TF32 "
+                    "filter_tensor_note": "executed on the tensor cores (rows of up to 2048 pixels, a multiple of 4): 3 TF32 "
                                           "products x 2 x rows x %d x %d per launch" % (wn, wk)},
         "clocks": clk.summary(),
     }
