@@ -5,10 +5,12 @@
 // Q^T = T G^T with T[j][k] = tau h[j - k].  A CTA computes a tile of 128
 // outputs j (the MMA's M, one TMEM lane each) by 128 rows r (its N, one TMEM
 // column each) and walks the row's inputs k in chunks of 32:
-//   * threads build the chunk's operands in shared memory in the canonical
-//     K-major 128-byte-swizzled layout: T from a tap table (the chunk of a
-//     Toeplitz matrix is a slice of the taps), G from the projections with the
-//     Feldkamp cosine weights applied;
+//   * 512 threads build the chunk's operands in shared memory in the
+//     canonical K-major 128-byte-swizzled layout with 16-byte stores: T from
+//     a tap table (a chunk of a Toeplitz matrix is a slice of the taps; four
+//     shifted copies make every four taps one aligned 16-byte load), G from
+//     the projections (loaded one chunk ahead) with the Feldkamp cosine
+//     weights applied;
 //   * one thread issues tcgen05.mma kind::tf32 (M 128, N 128, K 8) into FP32
 //     accumulators in TMEM; two stages, each released by tcgen05.commit on
 //     its mbarrier, let the next chunk be built while the MMAs run.
