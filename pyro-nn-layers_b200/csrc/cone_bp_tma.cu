@@ -228,7 +228,8 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
 #pragma unroll
     for (int z = 0; z < TB_Z; ++z) acc[z] = 0.0f;
     const float fi = (float)i, fj = (float)j, fk = (float)k0;
-    constexpr unsigned MAX_IDX = BOX_ELEMS - BOX_W - 2;
+    constexpr unsigned MAX_IDX = BOX_ELEMS - BOX_W - 2, MAX_IDX2 = BOX_ELEMS - 2 * BOX_W - 2;
+    static_assert(TB_Z % 2 == 0, "the column loop takes voxels in pairs");
 
     for (int p = 0; p < n_pass; ++p) {
         const int cur = p & 1, nxt = cur ^ 1;
@@ -259,14 +260,34 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
                 // row of floor(lv) from its FloorFrac bits: the bias folded into one offset
                 const unsigned col = (unsigned)fu.i - (unsigned)FLOOR_BIAS * (unsigned)BOX_W;
                 const float lv0 = fmaf(vb, rw, -m.v0), dlv = r1.z * rw;  // local v at z = 0, its step
+                if (dlv >= 0.0f && dlv < 0.999f) {
+                    // rows of voxels z and z + 1 differ by 0 or 1: the pair
+                    // reads rows r, r + 1, r + 2 once (three u lerps for two
+                    // voxels instead of four) and gives each voxel the same
+                    // taps, hence the same bits, as the loop below
 #pragma unroll
-                for (int z = 0; z < TB_Z; ++z) {
-                    const float lv = fmaf((float)z, dlv, lv0);
-                    const FloorFrac fv = floor_frac(lv);
-                    unsigned idx = (unsigned)fv.bits * (unsigned)BOX_W + col;
-                    idx = min(idx, MAX_IDX);  // memory safety only: the margin keeps idx in range
-                    const float val = lerp_ref(smem_ulerp(tile + idx, tx), smem_ulerp(tile + idx + BOX_W, tx), fv.f);
-                    acc[z] = fmaf(val, rw2, acc[z]);
+                    for (int z = 0; z < TB_Z; z += 2) {
+                        const float la = fmaf((float)z, dlv, lv0), lb = fmaf((float)(z + 1), dlv, lv0);
+                        const FloorFrac fa = floor_frac(la), fb = floor_frac(lb);
+                        unsigned idx = (unsigned)fa.bits * (unsigned)BOX_W + col;
+                        idx = min(idx, MAX_IDX2);  // memory safety only: the margin keeps idx in range
+                        const float p0 = smem_ulerp(tile + idx, tx), p1 = smem_ulerp(tile + idx + BOX_W, tx);
+                        const float p2 = smem_ulerp(tile + idx + 2 * BOX_W, tx);
+                        acc[z] = fmaf(lerp_ref(p0, p1, fa.f), rw2, acc[z]);
+                        const bool up = fb.bits != fa.bits;
+                        acc[z + 1] = fmaf(lerp_ref(up ? p1 : p0, up ? p2 : p1, fb.f), rw2, acc[z + 1]);
+                    }
+                } else {
+#pragma unroll
+                    for (int z = 0; z < TB_Z; ++z) {
+                        const float lv = fmaf((float)z, dlv, lv0);
+                        const FloorFrac fv = floor_frac(lv);
+                        unsigned idx = (unsigned)fv.bits * (unsigned)BOX_W + col;
+                        idx = min(idx, MAX_IDX);  // memory safety only: the margin keeps idx in range
+                        const float val =
+                            lerp_ref(smem_ulerp(tile + idx, tx), smem_ulerp(tile + idx + BOX_W, tx), fv.f);
+                        acc[z] = fmaf(val, rw2, acc[z]);
+                    }
                 }
             } else if (mode == MODE_SMEM) {
                 const T *tile = &tiles[cur][k][0];
