@@ -25,7 +25,9 @@ ORACLE_SRC = os.path.join(HERE, "oracle.c")
 ORACLE_LIB = os.path.join(HERE, "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 REF_LIB = os.path.join(REF_DIR, "libpyronn_ref.so")
-REF_SOURCES = "/root/reference/cc/kernels"
+# root of a PYRO-NN-Layers checkout whose cc/kernels/ build_ref compiles; no
+# default: without it build_ref keeps an existing _ref/ library
+REF_ROOT_ENV = "PYRONN_REFERENCE_ROOT"
 REF_FILES = [
     "par_projector_2D_CudaKernel.cu.cc",
     "par_backprojector_2D_CudaKernel.cu.cc",
@@ -47,11 +49,20 @@ def build_oracle(force=False) -> str:
     return ORACLE_LIB
 
 
-def build_ref(force=False, src_dir=REF_SOURCES) -> str | None:
+def reference_kernel_dir(root=None):
+    """cc/kernels of the reference checkout given by `root` or by the
+    PYRONN_REFERENCE_ROOT environment variable; None when neither is set."""
+    root = root or os.environ.get(REF_ROOT_ENV)
+    return os.path.join(root, "cc", "kernels") if root else None
+
+
+def build_ref(force=False, root=None) -> str | None:
     """Compiles the reference's 8 kernel files unmodified (BUILD:44 flags:
-    -DGOOGLE_CUDA=1, ftz=true) for sm_100a into _ref/.  Returns None when the
-    reference sources are not present (e.g. on a GPU box)."""
-    if not os.path.isdir(src_dir):
+    -DGOOGLE_CUDA=1, ftz=true) for sm_100a into _ref/, reading them where they
+    lie under `root` (default: $PYRONN_REFERENCE_ROOT).  Without the reference
+    sources (e.g. on a GPU box) it returns the existing library, or None."""
+    src_dir = reference_kernel_dir(root)
+    if src_dir is None or not os.path.isdir(src_dir):
         return REF_LIB if os.path.exists(REF_LIB) else None
     if os.path.exists(REF_LIB) and not force:
         return REF_LIB

@@ -560,7 +560,7 @@ static void bp3d_item(void *vctx, long item)
 }
 
 /* ConeBackprojection3D: cone_backprojector_3D_CudaKernel.cu.cc:84-118
- * (hardware_interp=0) and cone_backprojector_3D_CudaKernel_hardware_interp.cu.cc:202-234 (=1). */
+ * (hardware_interp=0) and cone_backprojector_3D_CudaKernel_hardware_interp.cu.cc:55-87 (=1). */
 void oracle_cone_backprojection3d(const float *sino, double *vol, int hardware_interp, int batch, int n_proj, int H,
                                   int W, int Z, int Y, int X, const float *vol_origin, const float *vol_spacing,
                                   const float *P, const float *mult, int geom_batch, int nthreads)

@@ -12,7 +12,7 @@
 // texel, y == H the next view's first row); a tap past the end of the
 // sinogram buffer -- undefined behaviour in the reference -- reads zero.
 // Hardware interpolation samples a layered texture at (u + 0.5, v + 0.5, n)
-// with border addressing, as cone_backprojector_3D_CudaKernel_hardware_interp.cu.cc:221-229.
+// with border addressing, as cone_backprojector_3D_CudaKernel_hardware_interp.cu.cc:81,115-119.
 #include "common.cuh"
 #include "internal.h"
 

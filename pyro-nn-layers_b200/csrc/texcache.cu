@@ -3,7 +3,7 @@
 // Texture filtering needs the data in a CUDA array.  The reference allocates
 // a fresh array, copies the whole input into it and frees it on every call
 // (cone_projector_3D_CudaKernel_hardware_interp.cu.cc:221-243,258;
-// cone_backprojector_3D_CudaKernel_hardware_interp.cu.cc:268-306).  Here the
+// cone_backprojector_3D_CudaKernel_hardware_interp.cu.cc:129-142,159).  Here the
 // arrays are kept in a per-device cache keyed by kind/extent/texel format and
 // handed out stream-aware: an entry is reused on the stream that used it last
 // (stream order makes that safe) or on any stream once the event recorded

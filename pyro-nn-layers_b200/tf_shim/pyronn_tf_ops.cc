@@ -3,10 +3,11 @@
 // inputs, attrs and shape functions, so graphs written against
 // PYRO-NN-Layers load this library instead (tf.load_op_library).
 //
-// Build (needs TensorFlow headers; not built in this repository's CI):
+// Build (needs TensorFlow headers; tests/test_tf_shim_cpu.py compile-checks this
+// file against stub declarations of the TensorFlow names it uses), one command:
 //   TF_CFLAGS=$(python -c 'import tensorflow as tf; print(" ".join(tf.sysconfig.get_compile_flags()))')
 //   TF_LFLAGS=$(python -c 'import tensorflow as tf; print(" ".join(tf.sysconfig.get_link_flags()))')
-//   g++ -std=c++17 -shared -fPIC pyronn_tf_ops.cc -o _pyronn_layers_ops.so $TF_CFLAGS $TF_LFLAGS \
+//   g++ -std=c++17 -shared -fPIC pyronn_tf_ops.cc -o _pyronn_layers_ops.so $TF_CFLAGS $TF_LFLAGS
 //       -I../../include -DGOOGLE_CUDA=1 -I/usr/local/cuda/include -L../pyronn_layers -lpyronn_b200
 //
 // Differences from the reference op kernels, all invisible to graph code:
@@ -188,7 +189,7 @@ class Op2D : public OpKernel {
         Tensor ws;
         const size_t ws_bytes = kForward ? pyronn_projection2d_workspace_size(batch, vol_y, vol_x, PYRONN_FLOAT32) : 0;
         if (ws_bytes)
-            OP_REQUIRES_OK(ctx, ctx->allocate_temp(DT_UINT8, TensorShape({(int64)ws_bytes}), &ws));
+            OP_REQUIRES_OK(ctx, ctx->allocate_temp(DT_UINT8, TensorShape({(int64_t)ws_bytes}), &ws));
         void *ws_ptr = ws_bytes ? (void *)ws.flat<uint8>().data() : nullptr;
         const float *p_vo = vo.flat<float>().data(), *p_do = dor.flat<float>().data();
         const float *p_vs = vs.flat<float>().data(), *p_ds = ds.flat<float>().data();
@@ -254,19 +255,24 @@ class OpCone : public OpKernel {
         const TensorShape os = kForward ? TensorShape({batch, n_proj, det_h, det_w})
                                         : TensorShape({batch, vol_z, vol_y, vol_x});
         OP_REQUIRES_OK(ctx, ctx->allocate_output(0, os, &out));
-        const size_t ws_bytes = kForward ? pyronn_cone_projection3d_workspace_size(g, n_proj)
-                                         : pyronn_cone_backprojection3d_workspace_size(g, n_proj);
+        const int hw = hardware_interp_ ? 1 : 0;
+        const size_t ws_bytes =
+            kForward ? pyronn_cone_projection3d_workspace_size(batch, vol_z, vol_y, vol_x, n_proj, det_h, det_w,
+                                                               PYRONN_FLOAT32, hw, g)
+                     : pyronn_cone_backprojection3d_workspace_size(batch, n_proj, det_h, det_w, vol_z, vol_y, vol_x,
+                                                                   PYRONN_FLOAT32, hw, g);
+        OP_REQUIRES(ctx, ws_bytes > 0, errors::InvalidArgument(name(), ": invalid problem size"));
         Tensor ws;
         OP_REQUIRES_OK(ctx, ctx->allocate_temp(DT_UINT8, TensorShape({(int64_t)ws_bytes}), &ws));
         const int st =
             kForward ? pyronn_cone_projection3d(in.flat<float>().data(), out->flat<float>().data(), PYRONN_FLOAT32,
-                                                PYRONN_FLOAT32, hardware_interp_ ? 1 : 0, batch, vol_z, vol_y, vol_x,
+                                                PYRONN_FLOAT32, hw, batch, vol_z, vol_y, vol_x,
                                                 n_proj, det_h, det_w, vo.flat<float>().data(), vs.flat<float>().data(),
                                                 P.flat<float>().data(), step.flat<float>().data(),
                                                 mult.flat<float>().data(), g, ws.flat<uint8>().data(), ws_bytes,
                                                 StreamOf(ctx))
                      : pyronn_cone_backprojection3d(in.flat<float>().data(), out->flat<float>().data(),
-                                                    PYRONN_FLOAT32, PYRONN_FLOAT32, hardware_interp_ ? 1 : 0, batch,
+                                                    PYRONN_FLOAT32, PYRONN_FLOAT32, hw, batch,
                                                     n_proj, det_h, det_w, vol_z, vol_y, vol_x,
                                                     vo.flat<float>().data(), vs.flat<float>().data(),
                                                     P.flat<float>().data(), step.flat<float>().data(),

@@ -3,7 +3,8 @@
     python tests/golden/make_golden.py [--out DIR]     (needs a CUDA GPU)
 
 Runs the reference's own CUDA launchers (cc/kernels/*.cu.cc of PYRO-NN-Layers,
-compiled unmodified into oracle/_ref/libpyronn_ref.so by oracle.build_ref())
+compiled unmodified into oracle/_ref/libpyronn_ref.so by oracle.build_ref(),
+with PYRONN_REFERENCE_ROOT set to the reference checkout)
 on small seeded inputs through oracle/ref/ref_driver.cu, which restates the
 TF op layer (per-batch-element launcher loop; FP64 projection-matrix
 decomposition rounded to FP32).  Each fixture stores the inputs, the geometry
@@ -62,7 +63,8 @@ def ptr(t):
 def load_ref():
     path = oracle.build_ref()
     if path is None or not os.path.exists(path):
-        raise SystemExit("oracle/_ref/libpyronn_ref.so missing: build it where the reference sources exist")
+        raise SystemExit("oracle/_ref/libpyronn_ref.so missing: build it where the reference sources exist "
+                         "(PYRONN_REFERENCE_ROOT=<checkout> python -c 'import oracle; oracle.build_ref()')")
     return ctypes.CDLL(path)
 
 
