@@ -65,6 +65,16 @@ PHANTOM_ELLIPSOIDS = 32
 NCU_DRAM_BYTES = {
     ("cone512", "fp16", "fp16", False): 37.972e9 + 0.574e9,
 }
+# ncu counters of the forward kernel (profiles/cone_fp_padded_kernel_cone256_fp16.md,
+# a --set full capture at 256^3): issue activity, and L2 -> SM bytes per ray
+# sample scaled to a 512^3 launch by its sample count
+NCU_FORWARD_COUNTERS = {
+    ("cone512", "fp16", "fp16", False): {
+        "issue_active": 0.829, "lanes_active_per_warp_instruction": 26.95,
+        "thread_instructions_per_sample": 46.7, "lts2xbar_bytes_per_sample_256": 11.0,
+        "source": "profiles/cone_fp_padded_kernel_cone256_fp16.md (256^3 capture; L2 -> SM bytes scale with "
+                  "the samples)"},
+}
 # kernels of ours launched per fwd+back step (geometry preparation, view
 # classification, the two volume copies, forward; preparation, backprojection)
 LAUNCHES_PER_STEP = {False: 7, True: 6}
@@ -208,6 +218,189 @@ def physical_gpu_index(local_rank):
     return str(local_rank)
 
 
+def sample_spec(cfg):
+    """The oracle's bounded sample of a step: (views, first z-slice, slices)."""
+    n_views, n_slices = 1, 2
+    return n_views, cfg["volume"][0] // 2 - n_slices // 2, n_slices
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+def host_in_bytes(cfg):
+    """Bytes of the FP32 host volume the e2e leg uploads per step."""
+    z, y, x = cfg["volume"]
+    return z * y * x * 4
+
+
+L2_READ_KERNEL = r"""
+extern "C" __global__ void l2_read(const float4 *__restrict__ a, unsigned n4, unsigned passes, float *out)
+{
+    const unsigned stride = gridDim.x * blockDim.x;
+    float acc = 0.0f;
+    for (unsigned p = 0; p < passes; ++p) {
+        const unsigned shift = p * 65537u;  // each pass starts each thread elsewhere
+        for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+            const float4 v = __ldcg(a + (i + shift) % n4);  // L2, not L1
+            acc += (v.x + v.y) + (v.z + v.w);
+        }
+    }
+    if (acc == -1.0f) out[0] = acc;  // keeps the loads; the data is never -1 summed
+}
+"""
+
+
+def measure_l2_peak(dev, mib=32, passes=64, repeats=7):
+    """L2 -> SM read bandwidth, measured the way the HBM peak is (a simple
+    kernel, CUDA events, best of N): a 16-byte ld.global.cg sweep of a
+    `mib` MiB buffer that stays L2-resident, `passes` sweeps per launch, a
+    grid of 8 blocks of 512 threads per SM.  The kernel is compiled at run time
+    with NVRTC for this GPU; it is a measurement probe, not part of the
+    library."""
+    import ctypes
+
+    import torch
+    from cuda.bindings import driver, nvrtc
+
+    def ok(res):
+        err = res[0]
+        if int(err) != 0:
+            raise RuntimeError("L2 probe: %s" % (err,))
+        return res[1:] if len(res) > 2 else (res[1] if len(res) == 2 else None)
+
+    major, minor = torch.cuda.get_device_capability(dev)
+    prog = ok(nvrtc.nvrtcCreateProgram(L2_READ_KERNEL.encode(), b"l2_read.cu", 0, [], []))
+    arch = ("--gpu-architecture=sm_%d%d%s" % (major, minor, "a" if major >= 9 else "")).encode()
+    if int(nvrtc.nvrtcCompileProgram(prog, 1, [arch])[0]) != 0:
+        raise RuntimeError("L2 probe: NVRTC compilation failed")
+    size = ok(nvrtc.nvrtcGetCUBINSize(prog))
+    cubin = b" " * size
+    ok((nvrtc.nvrtcGetCUBIN(prog, cubin)[0], None))
+    torch.cuda.init()
+    with torch.cuda.device(dev):
+        torch.zeros(1, device=dev)  # the primary context is current
+        module = ok(driver.cuModuleLoadData(cubin))
+        fn = ok(driver.cuModuleGetFunction(module, b"l2_read"))
+        n4 = mib * (1 << 20) // 16
+        a = torch.rand(n4 * 4, device=dev)
+        out = torch.zeros(1, device=dev)
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        grid, block = 8 * sms, 512
+        args = (ctypes.c_void_p(a.data_ptr()), ctypes.c_uint(n4), ctypes.c_uint(passes), ctypes.c_void_p(out.data_ptr()))
+        argv = (ctypes.c_void_p * 4)(*[ctypes.addressof(x) for x in args])
+        stream = torch.cuda.current_stream(dev)
+
+        def launch():
+            ok((driver.cuLaunchKernel(fn, grid, 1, 1, block, 1, 1, 0, stream.cuda_stream, ctypes.addressof(argv), 0)[0],
+                None))
+
+        for _ in range(3):
+            launch()
+        best = 0.0
+        for _ in range(repeats):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            launch()
+            e.record(stream)
+            torch.cuda.synchronize(dev)
+            best = max(best, n4 * 16.0 * passes / (s.elapsed_time(e) / 1e3) / 1e9)
+        ok((driver.cuModuleUnload(module)[0], None))
+    return {"gbs": best, "how": "ld.global.cg sweeps of a %d MiB L2-resident buffer, %d sweeps per launch, grid "
+                                "8 x SMs x 512 threads, best of %d launches (NVRTC-compiled probe)"
+                                % (mib, passes, repeats)}
+
+
+def oracle_slab(cfg, geo, sino_np):
+    """FP64 oracle backprojection of the sample slices of one sinogram."""
+    import oracle
+    nv, z0, ns = sample_spec(cfg)
+    out = oracle.cone_backprojection3d_slab(sino_np, geo.volume_shape, z0, z0 + ns, geo.volume_origin,
+                                            geo.volume_spacing, geo.projection_matrices, geo.projection_multiplier)
+    return out[z0:z0 + ns]
+
+
+def reference_gpu(cfg, geo, vol32, dev, f_ms, b_ms, ours_fp32_gups, ours_gups, args):
+    """The reference's own CUDA kernels (cc/kernels/*.cu.cc built unmodified
+    into oracle/_ref by the oracle's recipe), run through the op-layer
+    restatement oracle/ref/ref_driver.cu -- one launcher call per op with its
+    per-call allocations and FP32 storage, the reference's
+    Cone_Projection_Kernel_Launcher (cone_projector_3D_CudaKernel.cu.cc:225-257)
+    and Cone_Backprojection3D_Kernel_Launcher
+    (cone_backprojector_3D_CudaKernel.cu.cc:121-146) -- on this workload,
+    timed with CUDA events on the default stream; outside our timed regions.
+    Also the relative L2 distance of our FP32 results from theirs."""
+    import ctypes
+
+    import torch
+
+    import oracle
+    if not os.path.exists(oracle.REF_LIB):
+        return {"unavailable": "oracle/_ref/libpyronn_ref.so not built (needs the reference sources)"}
+    if args.hardware_interp:
+        return {"unavailable": "timed for the software-interpolation workload only"}
+    L = ctypes.CDLL(oracle.REF_LIB)
+    Z, Y, X = cfg["volume"]
+    H, W = cfg["detector"]
+    n = cfg["views"]
+    keep = []
+
+    def dptr(a, slack=0):
+        a = np.ascontiguousarray(np.asarray(a, dtype=np.float32)).reshape(-1)
+        t = torch.zeros(a.size + slack, dtype=torch.float32, device=dev)
+        t[: a.size] = torch.from_numpy(a).to(dev)
+        keep.append(t)
+        return ctypes.c_void_p(t.data_ptr())
+
+    vo, vs, P, st, mu = (np.asarray(a, np.float32)[None] for a in geo.args())
+    g = [dptr(vo), dptr(vs), dptr(P), dptr(st), dptr(mu)]
+    vol = vol32[None].contiguous()
+    sino = torch.zeros(n * H * W + W + 8, dtype=torch.float32, device=dev)  # slack for its x == W taps
+    back = torch.zeros(Z * Y * X, dtype=torch.float32, device=dev)
+    fargs = (ctypes.c_void_p(vol.data_ptr()), ctypes.c_void_p(sino.data_ptr()), 0, 1, Z, Y, X, n, H, W, g[0], g[1],
+             g[2], g[3])
+    bargs = (ctypes.c_void_p(sino.data_ptr()), ctypes.c_void_p(back.data_ptr()), 0, 1, n, H, W, Z, Y, X, g[0], g[1],
+             g[2], g[4])
+
+    def timed(fn, reps=2):
+        rc = fn()
+        if rc != 0:
+            raise RuntimeError("reference launcher failed with CUDA error %d" % rc)
+        times = []
+        for _ in range(reps):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            fn()
+            e.record()
+            torch.cuda.synchronize()
+            times.append(s.elapsed_time(e))
+        return statistics.mean(times)
+
+    try:
+        fms = timed(lambda: L.ref_cone_projection3d(*fargs))
+        bms = timed(lambda: L.ref_cone_backprojection3d(*bargs))
+    except RuntimeError as exc:
+        return {"unavailable": str(exc)}
+    # our FP32 results on the same inputs, for the parity figure at this size
+    from pyronn_layers import ops
+    ours_s = ops.cone_projection3d(vol, geo.detector_shape, *geo.args())
+    e_f = rel_l2(ours_s.reshape(-1).cpu().numpy(), sino[: n * H * W].cpu().numpy())
+    ours_v = ops.cone_backprojection3d(sino[: n * H * W].reshape(1, n, H, W), geo.volume_shape, *geo.args())
+    e_b = rel_l2(ours_v.reshape(-1).cpu().numpy(), back.cpu().numpy())
+    gups = 2 * updates(cfg) / ((fms + bms) / 1e3) / 1e9
+    return {"value": gups, "unit": "GUPS", "forward_ms": fms, "backprojection_ms": bms,
+            "storage": "fp32 (the reference's only storage type)",
+            "ours_fp32_over_reference": ours_fp32_gups / gups, "ours_over_reference": ours_gups / gups,
+            "forward_over_reference": fms / f_ms, "backprojection_over_reference": bms / b_ms,
+            "ours_fp32_forward_rel_l2_vs_reference": e_f, "ours_fp32_backprojection_rel_l2_vs_reference": e_b,
+            "what": "the reference's own kernels (cc/kernels/*.cu.cc built unmodified for sm_100a) through a "
+                    "restatement of its TF op layer (oracle/ref/ref_driver.cu): FP32, per-call allocations and "
+                    "host-side matrix decomposition as the reference's ops do, default stream, 1 warm-up + 2 timed "
+                    "calls per op; forward/backprojection_over_reference compare against OUR headline kernels"}
+
+
 # ------------------------------------------------------------------ CPU legs
 
 
@@ -216,7 +409,7 @@ def cpu_sample(cfg, geo, vol_np, sino_np, target_s=8.0, threads=None):
     (gups, sample description, threads, outputs for the accuracy check)."""
     import oracle
     threads = threads or (os.cpu_count() or 1)
-    n_views, n_slices = 1, 2
+    n_views, z0, n_slices = sample_spec(cfg)
     Z = cfg["volume"][0]
     t0 = time.perf_counter()
     fwd, _ = oracle.cone_projection3d_views(vol_np, geo.detector_shape, 0, n_views, geo.volume_origin,
@@ -224,7 +417,6 @@ def cpu_sample(cfg, geo, vol_np, sino_np, target_s=8.0, threads=None):
                                             nthreads=threads)
     t_fwd = time.perf_counter() - t0
     t0 = time.perf_counter()
-    z0 = Z // 2 - n_slices // 2
     back = oracle.cone_backprojection3d_slab(sino_np, geo.volume_shape, z0, z0 + n_slices, geo.volume_origin,
                                              geo.volume_spacing, geo.projection_matrices,
                                              geo.projection_multiplier, nthreads=threads)
@@ -407,16 +599,34 @@ def run_ours(args, cfg):
         del step32
         torch.cuda.empty_cache()
 
-    # ---- end to end through the public API: pinned host volume in, FP32
-    # volume out, every step.  Steps run as a stream of volumes does: two
+    # ---- BF16 storage (the precision the metric names), same kernels
+    bf16 = None
+    if storage != torch.bfloat16:
+        step16, ev16, _, sino16, back16 = make_step(torch.bfloat16, torch.bfloat16, torch.float32)
+        ms16 = timed(lambda rec=False: step16(rec), args.steps, args.warmup, True)
+        bf16 = {"value": 2 * updates(cfg) * world * args.steps / (ms16 / 1e3) / 1e9, "unit": "GUPS",
+                "storage": "bf16 volume, bf16 sinogram, FP32 arithmetic, FP32 volume out",
+                "forward_ms": statistics.mean(a.elapsed_time(b) for a, b, _ in ev16),
+                "backprojection_ms": statistics.mean(b.elapsed_time(c) for _, b, c in ev16)}
+        nv, z0, ns = sample_spec(cfg)
+        bf16_outputs = (sino16[0, :nv].float().cpu().numpy(), sino16.float().cpu().numpy()
+                        if world == 1 and not args.no_cpu_baseline else None,
+                        back16[0, z0:z0 + ns].float().cpu().numpy())
+        del step16, sino16, back16
+        torch.cuda.empty_cache()
+
+    # ---- end to end through the public API: pinned FP32 host volume in, FP32
+    # volume out, every step.  Each step uploads the FP32 volume, converts it
+    # to the storage dtype on the device, projects and backprojects, and
+    # downloads the FP32 result.  Steps run as a stream of volumes does: two
     # slots, the host->device copy of step i+1 and the device->host copy of
     # step i overlap step i's projections (copy engines, own streams); the
     # timed region ends when the last result is in host memory.
-    host_in = [torch.empty((1, Z, Y, X), dtype=storage, pin_memory=True) for _ in range(2)]
+    host_in = [torch.empty((1, Z, Y, X), dtype=torch.float32, pin_memory=True) for _ in range(2)]
     for h in host_in:
-        h.copy_(x.cpu())
+        h.copy_(vol32[None].cpu())
     host_out = [torch.empty((1, Z, Y, X), dtype=torch.float32, pin_memory=True) for _ in range(2)]
-    dev_in = [torch.empty_like(x) for _ in range(2)]
+    dev_in = [torch.empty((1, Z, Y, X), dtype=torch.float32, device=dev) for _ in range(2)]
     h2d, d2h = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
     comp = torch.cuda.current_stream(dev)
     slot_done = [None, None]
@@ -432,7 +642,8 @@ def run_ours(args, cfg):
                 ev_in = torch.cuda.Event()
                 ev_in.record(h2d)
             comp.wait_event(ev_in)
-            s = pl.cone_projection3d(dev_in[k], geo.detector_shape, *args_geo, hardware_interp=hw,
+            xs = dev_in[k].to(storage)
+            s = pl.cone_projection3d(xs, geo.detector_shape, *args_geo, hardware_interp=hw,
                                      out_dtype=sino_storage)
             b = pl.cone_backprojection3d(s, geo.volume_shape, *args_geo, hardware_interp=hw,
                                          out_dtype=torch.float32)
@@ -449,6 +660,7 @@ def run_ours(args, cfg):
     e2e_steps = max(8, args.steps)
     e2e_run(max(args.warmup, 3))
     torch.cuda.synchronize()
+    pl.check_device_errors(dev)
     barrier()
     e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e_start.record(comp)
@@ -465,28 +677,40 @@ def run_ours(args, cfg):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
     e2e_value = 2 * updates(cfg) * world * e2e_steps / (e2e_ms / 1e3) / 1e9
+    pl.check_device_errors(dev)  # a bounded device wait that gave up would void the run
+    del dev_in, host_in
+    torch.cuda.empty_cache()
 
-    # ---- roofline of the dominant kernel
+    # ---- roofline of the dominant kernel, against the L2 copy bandwidth
+    # measured here (the taps are served on chip; HBM traffic is `traffic`)
     es = 2 if storage != torch.float32 else 4
     es_s = 2 if sino_storage != torch.float32 else 4
     S = count_samples(cfg, dev)
     f_ms, b_ms = statistics.mean(fwd_ms), statistics.mean(back_ms)
     fwd_bytes = S * 8 * es + n_proj * H * W * es_s
     back_bytes = updates(cfg) * 4 * es_s + Z * Y * X * 4
-    peak, peak_kind = measured_peaks()
+    try:
+        l2 = measure_l2_peak(dev)
+    except Exception as exc:  # the probe needs NVRTC; report its absence instead of a number
+        l2 = {"gbs": None, "how": "L2 probe failed: %s" % exc}
+    hbm_peak, peak_kind = measured_peaks()
     if f_ms >= b_ms:
-        dom, dom_bytes, dom_ms = "cone_fp_kernel (forward)", fwd_bytes, f_ms
+        dom, dom_bytes, dom_ms = "cone_fp_padded_kernel (forward)", fwd_bytes, f_ms
     else:
-        dom, dom_bytes, dom_ms = "cone_bp_kernel (backprojection)", back_bytes, b_ms
+        dom, dom_bytes, dom_ms = "cone_bp_tma_kernel (backprojection)", back_bytes, b_ms
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": "%s HBM copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"
-                % peak_kind if peak_kind == "measured" else "fallback 6.65 TB/s",
-                "traffic": args.traffic_bytes if args.traffic_bytes is not None else NCU_DRAM_BYTES.get(
-                    (args.workload, args.storage, sino_storage_name(args), hw)) if f_ms >= b_ms else None,
+    ncu_key = (args.workload, args.storage, sino_storage_name(args), hw)
+    roofline = {"bound": "issue", "kernel": dom, "achieved": achieved, "peak": l2["gbs"], "unit": "GB/s",
+                "frac": achieved / l2["gbs"] if l2["gbs"] else None,
+                "peak_source": "L2 read bandwidth measured in this run (%s)" % l2["how"],
+                "traffic": args.traffic_bytes if args.traffic_bytes is not None else NCU_DRAM_BYTES.get(ncu_key)
+                if f_ms >= b_ms else None,
                 "algorithmic_bytes_per_launch": dom_bytes,
-                "note": "algorithmic bytes = interpolation taps x element size (+ output); frac > 1 means the "
-                        "gathers are served on chip, traffic (ncu dram bytes) is the HBM side"}
+                "hbm_peak": hbm_peak, "hbm_peak_source": "%s HBM copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"
+                % peak_kind if peak_kind == "measured" else "fallback 6.65 TB/s",
+                "ncu": NCU_FORWARD_COUNTERS.get(ncu_key) if f_ms >= b_ms else None,
+                "note": "algorithmic bytes = 8 taps x element size per ray sample (+ sinogram), over the live CUDA-event "
+                        "time; the limiter is instruction issue (ncu), not bytes: see ncu.issue_active"}
 
     line = {
         "metric": METRIC, "value": value, "unit": "GUPS", "n_gpus": world, "steps": args.steps,
@@ -496,14 +720,16 @@ def run_ours(args, cfg):
         "config": config_block(args, cfg),
         "plain_fp32_value": fp32_gups,
         "storage_over_fp32": (value / fp32_gups) if fp32_gups else None,
+        "bf16": bf16,
         "kernels": {"forward_ms": f_ms, "backprojection_ms": b_ms, "ray_samples": S,
                     "forward_gsamples_per_s": S / (f_ms / 1e3) / 1e9,
                     "backprojection_gups": updates(cfg) / (b_ms / 1e3) / 1e9},
         "roofline": roofline,
         "e2e": {"value": e2e_value, "unit": "GUPS",
-                "h2d_bytes_per_step": host_in[0].numel() * host_in[0].element_size(),
-                "d2h_bytes_per_step": host_out[0].numel() * host_out[0].element_size(), "steps": e2e_steps,
+                "h2d_bytes_per_step": host_in_bytes(cfg), "d2h_bytes_per_step": Z * Y * X * 4, "steps": e2e_steps,
                 "api": "pyronn_layers.cone_projection3d + cone_backprojection3d",
+                "input": "FP32 volume in pinned host memory, converted to the storage dtype on the device inside "
+                         "the timed region",
                 "overlap": "two slots: the H2D copy of step i+1 and the D2H copy of step i run on their own "
                            "streams during step i's projections; every step's input and result cross the host "
                            "link inside the timed region"},
@@ -511,25 +737,34 @@ def run_ours(args, cfg):
         "clocks": clocks,
     }
 
-    # ---- CPU baseline (rank 0, N = 1) and accuracy against the FP64 oracle
+    # ---- baselines (rank 0, N = 1): the CPU oracle on a bounded sample, the
+    # accuracy of the GPU results against it, and the reference's own CUDA
+    # kernels built from its sources -- all outside the timed regions
     if world == 1 and not args.no_cpu_baseline:
         vol_np = vol32.cpu().numpy()[None]
         sino_np = sino.float().cpu().numpy()
         gups, desc, threads, outs = cpu_sample(cfg, geo, vol_np, sino_np)
         line["cpu_baseline"] = {"value": gups, "unit": "GUPS", "cores": threads, "kind": "port", "sample": desc}
-        nv, z0, ns = outs["n_views"], outs["z0"], outs["n_slices"]
+        nv, z0, ns = sample_spec(cfg)
         ours_f = sino[0, :nv].float().cpu().numpy()
         ours_b = back[0, z0:z0 + ns].float().cpu().numpy()
-
-        def rel(a, b):
-            return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
-
         line["accuracy"] = {
-            "forward_rel_l2_vs_fp64": rel(ours_f, outs["fwd"]),
-            "backprojection_rel_l2_vs_fp64": rel(ours_b, outs["back"]),
+            "forward_rel_l2_vs_fp64": rel_l2(ours_f, outs["fwd"]),
+            "backprojection_rel_l2_vs_fp64": rel_l2(ours_b, outs["back"]),
             "note": "forward: %s storage of the FP32 phantom, %s sinogram, vs the FP64 oracle on the FP32 "
                     "phantom (%d view); backprojection: same sinogram, FP32 volume, %d z-slices"
                     % (args.storage, sino_storage_name(args), nv, ns)}
+        if bf16 is not None:
+            f16, s16_all, b16 = bf16_outputs
+            ref_b16 = oracle_slab(cfg, geo, s16_all)
+            bf16["forward_rel_l2_vs_fp64"] = rel_l2(f16, outs["fwd"])
+            bf16["backprojection_rel_l2_vs_fp64"] = rel_l2(b16, ref_b16)
+            bf16["fwd_back_rel_l2_bound"] = 1e-3
+            bf16["note"] = ("forward: BF16 storage of the FP32 phantom and a BF16 sinogram vs the FP64 oracle on the "
+                            "FP32 phantom; the rounding of BF16 storage alone (2^-9 relative, RMS 1.1e-3 for "
+                            "uniform rounding) exceeds the 1e-3 bound; FP16 storage meets it (accuracy above)")
+        del sino_np
+        line["reference_gpu"] = reference_gpu(cfg, geo, vol32, dev, f_ms, b_ms, fp32_gups or value, value, args)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
@@ -575,6 +810,72 @@ def run_serving(args):
         "serving": s_srv.as_dict(),
         "server_startup_s": warmup_s,
         "plain_one_job_per_launch_fp32": s_plain.as_dict(),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+
+
+def run_serving_sweep(args):
+    """Serving capacity (config 5's mix): the same seeded trace at stepped
+    Poisson rates and closed-loop (every request queued at t = 0), through the
+    continuous-batching server and through the plain one-job-per-launch FP32
+    path on the same GPU.  Per rate: offered and achieved GUPS, p50 / p99
+    latency.  Reported: each path's saturation GUPS (closed loop), the highest
+    rate whose achieved GUPS keeps up with the offered load (within 5 %), and
+    the highest rate whose p99 stays under the stated bound."""
+    import torch
+
+    from pyronn_layers import serving
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    geos = serving.standard_geometries()
+    rates = [float(r) for r in args.rates.split(",")]
+    p99_bound_ms = args.p99_bound_ms
+    classes = sorted({c for _, c in serving.poisson_trace(args.requests, 100.0, seed=7)}, key=str)
+    server = serving.ProjectorServer(geos, device=dev, keep_results=False)
+    warmup_s = server.warmup(classes, batch_sizes=(1, 2, 4, 8))
+    warm = serving.make_jobs([(0.0, c) for c in classes], geos, seed=1)
+    server.run_trace(warm, realtime=False)
+    serving.run_plain(serving.make_jobs([(0.0, c) for c in classes], geos, seed=1), geos, device=dev,
+                      realtime=False)
+    rows = []
+    with ClockSampler(physical_gpu_index(dev.index or 0)) as clk:
+        for rate in rates:
+            trace = serving.poisson_trace(args.requests, rate, seed=7)
+            mean_updates = float(np.mean([geos[c.geometry].updates for _, c in trace]))
+            offered = rate * mean_updates / 1e9 if math.isfinite(rate) else None
+            server.batches, server.batch_sizes = 0, []
+            jobs = serving.make_jobs(trace, geos, seed=1)
+            s_srv = server.run_trace(jobs, realtime=True)
+            jobs_plain = serving.make_jobs(trace, geos, seed=1)
+            s_plain = serving.run_plain(jobs_plain, geos, device=dev, realtime=True, keep_results=False)
+            rows.append({"rate_hz": rate if math.isfinite(rate) else "closed-loop", "offered_gups": offered,
+                         "server": {"gups": s_srv.gups, "p50_ms": s_srv.p50_ms, "p99_ms": s_srv.p99_ms,
+                                    "mean_batch": s_srv.mean_batch},
+                         "plain": {"gups": s_plain.gups, "p50_ms": s_plain.p50_ms, "p99_ms": s_plain.p99_ms}})
+
+    def summary(path):
+        fin = [r for r in rows if r["offered_gups"] is not None]
+        closed = [r[path]["gups"] for r in rows if r["offered_gups"] is None]
+        keeps = [r["rate_hz"] for r in fin if r[path]["gups"] >= 0.95 * r["offered_gups"]]
+        under = [r["rate_hz"] for r in fin if r[path]["p99_ms"] <= p99_bound_ms]
+        return {"saturation_gups": max(closed) if closed else None,
+                "max_sustained_gups": max([r[path]["gups"] for r in fin if r["rate_hz"] in keeps], default=None),
+                "highest_rate_keeping_up_hz": max(keeps, default=None),
+                "highest_rate_p99_under_bound_hz": max(under, default=None)}
+
+    srv, plain = summary("server"), summary("plain")
+    line = {
+        "metric": METRIC, "value": srv["saturation_gups"] or srv["max_sustained_gups"], "unit": "GUPS", "n_gpus": 1,
+        "steps": args.requests * len(rates), "warmup": 1, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "storage": "fp32/bf16 mix", "data": "synthetic",
+        "config": {"workload": "serving-sweep", "requests_per_rate": args.requests, "rates_hz": args.rates,
+                   "p99_bound_ms": p99_bound_ms,
+                   "mix": "60% fan 512^2 (360 views, 1024 px), 30% cone 128^3 (180 views, 256^2), 10% cone 256^3 "
+                          "(360 views, 512^2); forward/back 50/50; FP32/BF16 50/50",
+                   "arrivals": "Poisson, seed 7; closed-loop: every request queued at t = 0"},
+        "server": srv, "plain_one_job_per_launch_fp32": plain, "rows": rows, "server_startup_s": warmup_s,
         "clocks": clk.summary(),
     }
     print(json.dumps(line))
@@ -653,6 +954,134 @@ def run_fan2d(args):
                    "sdd_mm": c["sdd_mm"], "phantom": "10 seeded ellipses per slice"},
         "plain_fp32_value": gups32,
         "kernels": {"forward_ms": f_ms, "backprojection_ms": b_ms},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+
+
+DIFFCONE = dict(batch=4, volume=(128, 128, 128), voxel_mm=1.0, views=180, detector=(256, 256), pixel_mm=1.5,
+                sid_mm=600.0, sdd_mm=1000.0, i0=1e5, unrolled=20)
+
+
+def run_diffcone(args):
+    """Differentiable cone beam (config 4): a batch of 4 volumes of 128^3 at
+    1.0 mm, 180 views over 2 pi, 256 x 256 detector at 1.5 mm, SID 600 / SDD
+    1000; y = -log(Poisson(1e5 exp(-A x_true)) / 1e5); one training step =
+    20 unrolled gradient steps x <- x - lr_k A^T (A x - y) from x = 0 (each
+    wrapped in activation checkpointing), the loss 1/2 |A x_20 - y|^2, its
+    backward pass through every step (checkpointed steps recomputed) and an
+    Adam update of the 20 learned step lengths.  The projector's gradient is
+    the exact transpose (matched adjoint) unless --unmatched.  GUPS = projector
+    and backprojector calls per training step (counted) x 4 x 128^3 x 180 / t.
+    Reported with and without checkpointing: time per step and peak memory."""
+    import torch
+
+    from pyronn_layers import geometry, ops, phantoms, recon
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    c = DIFFCONE
+    geo = geometry.ConeBeam3D(c["volume"], (c["voxel_mm"],) * 3, c["detector"], (c["pixel_mm"],) * 2, c["views"],
+                              c["sid_mm"], c["sdd_mm"])
+    vols = np.stack([phantoms.ellipsoid_phantom_3d(c["volume"], geo.volume_spacing, seed=400 + b)[0]
+                     for b in range(c["batch"])]) * np.float32(0.02)
+    x_true = torch.from_numpy(vols).to(dev)
+    y_dev = recon.poisson_sinogram(ops.cone_projection3d(x_true, geo.detector_shape, *geo.args()), c["i0"], seed=4)
+    y_host = y_dev.cpu().pin_memory()
+    units = c["batch"] * int(np.prod(c["volume"])) * c["views"]
+
+    def step_length(matched):
+        """1 / the largest eigenvalue of A^T A (power iteration, 12 steps):
+        the step that keeps the unrolled descent stable, the learned step
+        lengths' starting value."""
+        x = torch.rand_like(x_true)
+        lam = 1.0
+        with torch.no_grad():
+            for _ in range(12):
+                ax = ops.cone_projection3d(x, geo.detector_shape, *geo.args())
+                atax = (ops.cone_backprojection3d_matched(ax, geo.volume_shape, *geo.args()) if matched
+                        else ops.cone_backprojection3d(ax, geo.volume_shape, *geo.args()))
+                lam = float(atax.norm() / x.norm())
+                x = atax / atax.norm()
+        return 1.0 / lam
+
+    calls = {"n": 0}
+    counted = {}
+    for name in ("_run_cone", "_run_matched"):
+        fn = getattr(ops, name)
+
+        def wrap(*a, _fn=fn, **k):
+            calls["n"] += 1
+            return _fn(*a, **k)
+        counted[name] = fn
+        setattr(ops, name, wrap)
+
+    def run(ckpt, steps, warmup, matched, lr0):
+        net = recon.UnrolledGradientDescent(geo, n_steps=c["unrolled"], init_lr=lr0, matched_adjoint=matched,
+                                            checkpoint=ckpt).to(dev)
+        opt = torch.optim.Adam(net.parameters(), lr=1e-2)
+        y = torch.empty_like(y_dev)
+        losses = []
+
+        def step():
+            y.copy_(y_host, non_blocking=True)  # this step's target sinogram from pinned host memory
+            opt.zero_grad(set_to_none=True)
+            xk = net(torch.zeros_like(x_true), y)
+            r = ops.cone_projection3d(xk, geo.detector_shape, *geo.args(), matched_adjoint=matched) - y
+            loss = 0.5 * (r.double() ** 2).sum()
+            loss.backward()
+            opt.step()
+            losses.append(loss.detach().to("cpu", non_blocking=True))  # the step's result back on the host
+
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        ops.check_device_errors(dev)
+        torch.cuda.reset_peak_memory_stats(dev)
+        calls["n"] = 0
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(steps):
+            step()
+        e.record()
+        torch.cuda.synchronize()
+        ops.check_device_errors(dev)
+        return {"ms_per_step": s.elapsed_time(e) / steps, "calls_per_step": calls["n"] / steps,
+                "peak_mem_gib": torch.cuda.max_memory_allocated(dev) / 2 ** 30,
+                "loss_first": float(losses[0]), "loss_last": float(losses[-1])}
+
+    try:
+        lr_u, lr_m = step_length(False), step_length(True)
+        with ClockSampler(physical_gpu_index(dev.index or 0)) as clk:
+            ck = run(True, args.steps, args.warmup, False, lr_u)
+        plain = run(False, max(1, args.steps // 2), 1, False, lr_u)
+        exact = run(True, 2, 1, True, lr_m)
+    finally:
+        for name, fn in counted.items():
+            setattr(ops, name, fn)
+    gups = ck["calls_per_step"] * units / (ck["ms_per_step"] / 1e3) / 1e9
+    ck["initial_step_length"], exact["initial_step_length"] = lr_u, lr_m
+    exact["gups"] = exact["calls_per_step"] * units / (exact["ms_per_step"] / 1e3) / 1e9
+    line = {
+        "metric": "differentiable cone-beam training step (config 4) GUPS", "value": gups, "unit": "GUPS",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ck["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "storage": "fp32",
+        "data": "synthetic (seeded ellipsoid phantoms, Poisson noise)",
+        "config": {"workload": "diffcone", "batch": c["batch"], "volume": list(c["volume"]), "voxel_mm": c["voxel_mm"],
+                   "views": c["views"], "detector_hw": list(c["detector"]), "pixel_mm": c["pixel_mm"],
+                   "sid_mm": c["sid_mm"], "sdd_mm": c["sdd_mm"], "i0": c["i0"], "unrolled_steps": c["unrolled"],
+                   "adjoint": "the reference's pairing: the voxel-driven backprojector as the projector's gradient "
+                              "(exact transpose: see exact_adjoint)",
+                   "optimizer": "Adam on the 20 learned step lengths"},
+        "checkpointed": ck, "no_checkpointing": plain,
+        "exact_adjoint": dict(exact, note="the same training step with the matched (exact-transpose, atomic "
+                                          "scatter) backprojector as gradient and in the unrolled steps; 1 warm-up "
+                                          "+ 2 timed steps"),
+        "updates_per_op": units,
+        "e2e": {"value": gups, "unit": "GUPS", "h2d_bytes_per_step": int(y_host.numel() * 4),
+                "d2h_bytes_per_step": 8,
+                "note": "the training step is timed through the public API with the target sinogram uploaded and "
+                        "the loss downloaded every step"},
         "clocks": clk.summary(),
     }
     print(json.dumps(line))
@@ -748,9 +1177,14 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving", "fan2d", "fdk"], default="cone512")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving", "serving-sweep", "fan2d", "fdk", "diffcone"],
+                    default="cone512")
+
     ap.add_argument("--requests", type=int, default=2000, help="serving: number of requests")
     ap.add_argument("--rate", type=float, default=100.0, help="serving: Poisson arrival rate (1/s)")
+    ap.add_argument("--rates", default="300,600,900,1200,1800,inf",
+                    help="serving-sweep: arrival rates (1/s; inf = closed loop)")
+    ap.add_argument("--p99-bound-ms", type=float, default=100.0, help="serving-sweep: the p99 latency bound")
     ap.add_argument("--storage", choices=["bf16", "fp16", "fp32"], default="fp16",
                     help="storage of the volume the forward projection reads (fp16: the 16-bit format that keeps "
                          "the forward within 1e-3 of the FP64 oracle; bf16 rounds piecewise-constant densities "
@@ -769,11 +1203,24 @@ def main(argv=None):
             return
         run_fan2d(args)
         return
+    if args.workload == "diffcone":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the training workload is measured on the GPU arm "
+                                                                   "only"}))
+            return
+        run_diffcone(args)
+        return
     if args.workload == "fdk":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no FDK filter"}))
             return
         run_fdk(args)
+        return
+    if args.workload == "serving-sweep":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the serving stream has no CPU reference arm"}))
+            return
+        run_serving_sweep(args)
         return
     if args.workload == "serving":
         if args.impl == "reference":

@@ -69,11 +69,29 @@ PYRONN_API const char *pyronn_status_string(int status);
 /* Detail of the last failing call on the calling host thread ("" if none). */
 PYRONN_API const char *pyronn_last_error(void);
 
-/* Reads the device error flag a cone call left in its workspace (0 = none,
- * 1 = a bounded wait for a TMA transfer timed out and the result is invalid).
+/* Device error flags (the kernels' bounded waits never hang: a wait that
+ * gives up records this, and the affected output is invalid). */
+#define PYRONN_DEVICE_ERROR_NONE 0
+#define PYRONN_DEVICE_ERROR_WAIT_TIMEOUT 1
+
+/* Reads the device error flag a cone call left in its workspace
+ * (PYRONN_DEVICE_ERROR_NONE, or PYRONN_DEVICE_ERROR_WAIT_TIMEOUT: a bounded
+ * wait for a TMA transfer timed out and the volume is invalid).
  * Synchronises the stream.  No counterpart in the reference (which has no
  * asynchronous error reporting). */
 PYRONN_API int pyronn_workspace_error(const void *workspace, void *stream, int *device_error);
+
+/* Testing hook, not for production use.  While enable != 0, every block of the
+ * TMA-staged cone backprojector (the software-interpolation path of
+ * pyronn_cone_backprojection3d and of pyronn_cone_backprojection3d_noalloc for
+ * 16-byte aligned detector rows) starves the bounded wait of its last pass of
+ * views: that pass issues no copy and waits, with a short spin limit, for
+ * bytes that never arrive.  The wait runs out and the call's device error
+ * flag becomes PYRONN_DEVICE_ERROR_WAIT_TIMEOUT (the volume is invalid).  No
+ * copy is in flight when the wait gives up, so the device stays usable.
+ * Process-wide; affects calls enqueued while it is set.  No counterpart in
+ * the reference. */
+PYRONN_API int pyronn_debug_starve_tma_wait(int enable);
 
 /* Frees the CUDA arrays the hardware_interp paths cached on the current
  * device.  Waits for the work that still reads them (device synchronise). */
@@ -178,7 +196,7 @@ PYRONN_API int pyronn_cone_projection3d(const void *volume, void *sinogram, int 
  * ConeBackprojection3D
  *   replaces REGISTER_OP("ConeBackprojection3D")       cc/ops/cone_backprojector_3D_OPKernel.cc:27-53,
  *   Cone_Backprojection3D_Kernel_Launcher              cc/kernels/cone_backprojector_3D_CudaKernel.cu.cc:121-146
- *   and Cone_Backprojection3D_Kernel_Tex_Interp_Launcher cc/kernels/cone_backprojector_3D_CudaKernel_hardware_interp.cu.cc:251-307
+ *   and Cone_Backprojection3D_Kernel_Tex_Interp_Launcher cc/kernels/cone_backprojector_3D_CudaKernel_hardware_interp.cu.cc:104-160
  *   sinogram [batch, n_proj, det_h, det_w] -> volume [batch, vol_z, vol_y, vol_x]
  *   step_size is accepted and unused, as in the reference.
  * ------------------------------------------------------------------------- */
@@ -239,6 +257,14 @@ PYRONN_API int pyronn_cone_backprojection3d_matched(const void *sinogram, float 
  * ------------------------------------------------------------------------- */
 #define PYRONN_NOALLOC_MAX_VIEWS 8192
 
+/* Reads the device error flag that the last
+ * pyronn_cone_backprojection3d_noalloc call on the current device left in the
+ * fixed scratch (PYRONN_DEVICE_ERROR_NONE, or
+ * PYRONN_DEVICE_ERROR_WAIT_TIMEOUT: the volume is invalid).
+ * Synchronises the stream; allocates nothing.  No counterpart in the
+ * reference. */
+PYRONN_API int pyronn_noalloc_error(void *stream, int *device_error);
+
 PYRONN_API int pyronn_cone_backprojection3d_noalloc(const void *sinogram, void *volume, int in_dtype,
                                                     int out_dtype, int batch, int n_proj, int det_h, int det_w,
                                                     int vol_z, int vol_y, int vol_x, const float *volume_origin,
@@ -298,6 +324,13 @@ PYRONN_API int pyronn_fdk_filter(const void *projections, void *filtered, int in
                                  int n_proj, int det_h, int det_w, double sdd, double det_spacing_v,
                                  double det_spacing_u, double principal_v, double principal_u, int filter,
                                  int weight_output, void *stream);
+
+/* Reads and clears the device error flag of the tensor-core filter on the
+ * current device: PYRONN_DEVICE_ERROR_WAIT_TIMEOUT if a bounded wait of any
+ * pyronn_fdk_filter call since the last read gave up (that call's rows of the
+ * affected tile were not written), else PYRONN_DEVICE_ERROR_NONE.
+ * Synchronises the stream. */
+PYRONN_API int pyronn_fdk_error(void *stream, int *device_error);
 
 #ifdef __cplusplus
 }

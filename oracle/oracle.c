@@ -249,10 +249,18 @@ static void fp2d_item(void *vctx, long item)
         double uu = (double)u * ds + dorg;
         double sx, sy, dx, dy;
         if (!c->fan) {
-            /* par_projector_2D_CudaKernel.cu.cc:120-132 */
-            double sid = sqrt((double)c->X * g.sx * (double)c->X * g.sx + (double)c->Y * g.sy * (double)c->Y * g.sy) * 1.2;
-            sx = rx * (-sid) + (-ry) * uu;
-            sy = ry * (-sid) + rx * uu;
+            /* par_projector_2D_CudaKernel.cu.cc:120-132: the virtual source
+             * point is formed in FP32 as the reference forms it (its sid, the
+             * detector coordinate, and ray * (-sid) + u_vec * u with the
+             * second product fused): a ray that grazes the box -- e.g. along
+             * an axis with a 1e-17 cross component -- enters or misses on
+             * that rounding */
+            float fsx = (float)g.sx, fsy = (float)g.sy, fX = (float)c->X, fY = (float)c->Y;
+            float fsid = sqrtf((fX * fsx * fX * fsx) + (fY * fsy * fY * fsy)) * 1.2f;
+            float fu = fmaf((float)u, (float)ds, (float)dorg);
+            float frx = (float)rx, fry = (float)ry;
+            sx = (double)fmaf(-fry, fu, frx * -fsid);
+            sy = (double)fmaf(frx, fu, fry * -fsid);
             dx = rx;
             dy = ry;
         } else {
@@ -320,6 +328,29 @@ static void intersect_lines(double p1x, double p1y, double p2x, double p2y, doub
     *oy = (a * (p3y - p4y) - (p1y - p2y) * bq) / dn;
 }
 
+/* Detector index of pixel (cx, cy) for a fan view by the reference's FP32
+ * steps (fan_backprojector_2D_CudaKernel.cu.cc:47-59 with intersectLines2D,
+ * helper_geometry_gpu.h:28-44), each operation rounded once (this file is
+ * built with -ffp-contract=off): near the source's depth the reference's FP32
+ * intersection is far from the exact one -- NaN below its 1e-6 threshold,
+ * which its texture samples as coordinate 0 (index -0.5), a far-off point
+ * just above.  The GPU kernel takes the same steps there. */
+static double fan_index_reference_steps(float cx, float cy, float rx, float ry, float sid, float sdd, float dorg,
+                                        float ds)
+{
+    float srcx = rx * -sid, srcy = ry * -sid;
+    float cpx = srcx + rx * sdd, cpy = srcy + ry * sdd;
+    float detx = -ry, dety = rx;
+    float p4x = cpx + detx, p4y = cpy + dety;
+    float a1 = cx - srcx, b1 = cpy - p4y, a2 = cy - srcy, b2 = cpx - p4x;
+    float dn = a1 * b1 - a2 * b2;
+    if (dn < 0.000001f && dn > -0.000001f) return -0.5;
+    float x12 = cx * srcy - cy * srcx, x34 = cpx * p4y - cpy * p4x;
+    float x = (x12 * b2 - a1 * x34) / dn, y = (x12 * b1 - a2 * x34) / dn;
+    float s = x * detx + y * dety;
+    return (double)((s - dorg) / ds);
+}
+
 static void bp2d_item(void *vctx, long item)
 {
     bp2d_ctx *c = (bp2d_ctx *)vctx;
@@ -353,6 +384,15 @@ static void bp2d_item(void *vctx, long item)
                 s = ix * dvx + iy * dvy;
             }
             double sidx = (s - dorg) / ds;
+            if (c->fan) {
+                /* within 1e-2 mm of the source's depth the reference's FP32
+                 * steps decide (see fan_index_reference_steps) */
+                double sid = c->sid[gb], sdd = c->sdd[gb];
+                double depth = (cx + rx * sid) * rx + (cy + ry * sid) * ry;
+                if (fabs(depth) < 1e-2)
+                    sidx = fan_index_reference_steps((float)cx, (float)cy, (float)rx, (float)ry, (float)sid, (float)sdd,
+                                                     (float)dorg, (float)ds);
+            }
             /* tex2D(s_idx + 0.5, n + 0.5): row n exactly, linear along u */
             acc += bilinear_border(sino, c->W, c->n_proj, sidx, (double)n) * w;
         }

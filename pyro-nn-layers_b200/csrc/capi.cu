@@ -227,6 +227,22 @@ const char *pyronn_last_error(void)
     return t_last_error.c_str();
 }
 
+int pyronn_debug_starve_tma_wait(int enable)
+{
+    cone_bp_tma_starve_last_pass(enable);
+    return ok();
+}
+
+int pyronn_fdk_error(void *stream, int *device_error)
+{
+    if (!device_error) return fail(PYRONN_ERROR_INVALID_ARGUMENT, "fdk_error: null pointer");
+    unsigned flag = 0;
+    cudaError_t e = fdk_tc_error((cudaStream_t)stream, &flag);
+    if (e != cudaSuccess) return cuda_fail(e, "fdk_error");
+    *device_error = (int)flag;
+    return ok();
+}
+
 int pyronn_release_cached_arrays(void)
 {
     const int freed = array_cache_clear();

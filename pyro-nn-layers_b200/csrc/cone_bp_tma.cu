@@ -4,11 +4,17 @@
 //
 // Block = 256 threads = 32 (x) x 8 (y) voxels, each thread walks 16 voxels
 // along z: a 32 x 8 x 16 voxel tile.  Views are processed in passes of
-// BP_K views.  For every view of a pass one warp projects the 8 tile corners,
+// BP_K views (BpViews).  For every view of a pass one warp (of four views) projects the 8 tile corners,
 // takes the bounding box of the taps the tile can touch (+1 pixel margin), and
 // one thread issues a 3D TMA load of a BW x BH detector box around it into
 // shared memory; the next pass's boxes load while the current pass computes
 // (two stages, one mbarrier per stage, bounded waits).
+// A wait that gives up records DEVICE_ERROR_MBARRIER_TIMEOUT in the error
+// word; the block then issues no further load and uses its barriers no more
+// (a phase that did not complete must not see another arrival), finishes its
+// passes on whatever the tiles hold, and before it exits waits (again
+// bounded) for the two passes that can still have boxes in flight.  Its
+// voxels are stored, invalid: the error word says so.
 //
 // Exactness: the tap indices and weights are computed exactly as the direct
 // path computes them (floor of u/w, frac), only the texel source differs.  TMA
@@ -27,6 +33,8 @@
 // v = (P1 . x) / w).
 #include <cuda.h>
 
+#include <atomic>
+
 #include "common.cuh"
 #include "internal.h"
 #include "tma.cuh"
@@ -35,10 +43,25 @@ namespace pyronn {
 
 namespace {
 
+#ifndef PYRONN_BP_PAIRS
+#define PYRONN_BP_PAIRS 0
+#endif
 constexpr int TB_X = 32;
 constexpr int TB_Y = 8;
 constexpr int TB_Z = 16;  // voxels per thread along z
-constexpr int BP_K = 4;  // views per pass
+#ifndef PYRONN_BP_K16
+#define PYRONN_BP_K16 4
+#endif
+constexpr int BP_K_MAX = 8;
+// views per pass: 4 for FP32 sinograms, PYRONN_BP_K16 for 16-bit ones (two
+// stages of K boxes must leave room for 4 blocks per SM)
+template <typename T>
+struct BpViews {
+    static constexpr int K = sizeof(T) == 2 ? PYRONN_BP_K16 : 4;
+    // a warp sets up four views; the last warp's surplus lanes set up views of
+    // the next pass into unused meta slots, which nothing reads
+    static_assert(K % 2 == 0 && K >= 4 && K <= BP_K_MAX, "views per pass");
+};
 constexpr int BOX_W = 72;  // 72-element rows shift banks between rows (64 would alias them)
 constexpr int BOX_H = 24;
 constexpr int BOX_ELEMS = BOX_W * BOX_H;
@@ -175,15 +198,18 @@ template <typename T, typename Tout>
 __global__ void __launch_bounds__(TB_X *TB_Y)
     cone_bp_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T *__restrict__ sino, Tout *__restrict__ vol,
                        const ConeBpView *__restrict__ views, const float *__restrict__ mult, int X, int Y, int Z,
-                       int W, int H, int n_proj, int geom_batch, unsigned *__restrict__ err)
+                       int W, int H, int n_proj, int geom_batch, unsigned *__restrict__ err,
+                       int starve_last_pass)
 {
     extern __shared__ __align__(128) unsigned char dyn_smem[];
     // TMA destinations must be 128-byte aligned: round the base up (the
     // launch reserves 128 spare bytes); every tile is a multiple of 128 bytes
     unsigned char *tile_base = dyn_smem + ((128u - (smem_addr(dyn_smem) & 127u)) & 127u);
+    constexpr int BP_K = BpViews<T>::K;
     T(*tiles)[BP_K][BOX_ELEMS] = reinterpret_cast<T(*)[BP_K][BOX_ELEMS]>(tile_base);  // [2][BP_K][BOX_ELEMS]
-    __shared__ __align__(16) ViewMeta meta[2][BP_K];
+    __shared__ __align__(16) ViewMeta meta[2][BP_K_MAX];
     __shared__ __align__(8) uint64_t full[2];
+    __shared__ int s_failed;  // first pass whose wait gave up, n_pass if none (kept out of registers)
 
     const int tid = threadIdx.y * TB_X + threadIdx.x;
     const int warp = tid >> 5;
@@ -203,9 +229,18 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
         mbar_init(&full[0], 1);
         mbar_init(&full[1], 1);
         fence_mbar_init();
+        s_failed = n_pass;
     }
+    // spin limit of the bounded waits: short for the starved test pass
+#define PYRONN_BP_SPINS (starve_last_pass ? (1u << 12) : (1u << 22))
     // issues the TMA loads of pass p into stage s (one thread)
     auto issue = [&](int p, int s) {
+        if (s_failed < n_pass) return;  // after a failed wait: no load, no arrival
+        if (starve_last_pass && p == n_pass - 1) {
+            // test hook: wait for bytes no copy will deliver, with no copy in flight
+            mbar_arrive_expect_tx(&full[s], 16u);
+            return;
+        }
         int n_fast = 0;
 #pragma unroll
         for (int k = 0; k < BP_K; ++k) n_fast += (p * BP_K + k < n_proj && meta[s][k].mode == MODE_SMEM);
@@ -217,9 +252,17 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
                 tma_load_3d(&tiles[s][k][0], &tmap, meta[s][k].iu0, meta[s][k].iv0, b * n_proj + n, &full[s]);
         }
     };
-    if (warp == 0) {
-        pass_meta<T>(meta[0], pv, 0, n_proj, i0, j0, k0, W, H);
-        __syncwarp();
+    // the warps that set up a pass's views (four each) meet before thread 0
+    // issues its loads
+    auto meta_ready = [&]() {
+        if (BP_K == 4)
+            __syncwarp();
+        else
+            asm volatile("bar.sync 1, %0;" ::"r"((BP_K + 3) / 4 * 32) : "memory");
+    };
+    if (warp < (BP_K + 3) / 4) {
+        pass_meta<T>(meta[0] + 4 * warp, pv, 4 * warp, n_proj, i0, j0, k0, W, H);
+        meta_ready();
     }
     __syncthreads();
     if (tid == 0) issue(0, 0);
@@ -234,12 +277,13 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
     for (int p = 0; p < n_pass; ++p) {
         const int cur = p & 1, nxt = cur ^ 1;
         __syncthreads();  // pass p-1 is done with stage nxt
-        if (warp == 0 && p + 1 < n_pass) {
-            pass_meta<T>(meta[nxt], pv, (p + 1) * BP_K, n_proj, i0, j0, k0, W, H);
-            __syncwarp();
+        if (warp < (BP_K + 3) / 4 && p + 1 < n_pass) {
+            pass_meta<T>(meta[nxt] + 4 * warp, pv, (p + 1) * BP_K + 4 * warp, n_proj, i0, j0, k0, W, H);
+            meta_ready();
             if (tid == 0) issue(p + 1, nxt);
         }
-        mbar_wait_bounded(&full[cur], (p >> 1) & 1, err);
+        if (s_failed == n_pass && !mbar_wait_bounded(&full[cur], (p >> 1) & 1, err, PYRONN_BP_SPINS))
+            atomicMin(&s_failed, p);
 #pragma unroll 1
         for (int k = 0; k < BP_K; ++k) {
             const int n = p * BP_K + k;
@@ -265,6 +309,29 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
                     // reads rows r, r + 1, r + 2 once (three u lerps for two
                     // voxels instead of four) and gives each voxel the same
                     // taps, hence the same bits, as the loop below
+#if PYRONN_BP_PAIRS
+                    // the pair's v, floors, v lerps and accumulations on
+                    // f32x2 values (sm_100 packed FP32): the same operations
+                    // on each half, so the same bits
+                    const float2 dlv2 = make_float2(dlv, dlv), lv02 = make_float2(lv0, lv0);
+                    const float2 rw22 = make_float2(rw2, rw2);
+#pragma unroll
+                    for (int z = 0; z < TB_Z; z += 2) {
+                        const float2 l = __ffma2_rn(make_float2((float)z, (float)(z + 1)), dlv2, lv02);
+                        const FloorFrac2 f = floor_frac2(l);
+                        unsigned idx = (unsigned)f.bits0 * (unsigned)BOX_W + col;
+                        idx = min(idx, MAX_IDX2);  // memory safety only: the margin keeps idx in range
+                        const float p0 = smem_ulerp(tile + idx, tx), p1 = smem_ulerp(tile + idx + BOX_W, tx);
+                        const float p2 = smem_ulerp(tile + idx + 2 * BOX_W, tx);
+                        const bool up = f.bits1 != f.bits0;
+                        const float2 lo = make_float2(p0, up ? p1 : p0), hi = make_float2(p1, up ? p2 : p1);
+                        const float2 nf = __ffma2_rn(f.f, make_float2(-1.0f, -1.0f), make_float2(0.0f, 0.0f));
+                        float2 a = make_float2(acc[z], acc[z + 1]);
+                        a = __ffma2_rn(lerp_ref2(lo, hi, f.f, nf), rw22, a);
+                        acc[z] = a.x;
+                        acc[z + 1] = a.y;
+                    }
+#else
 #pragma unroll
                     for (int z = 0; z < TB_Z; z += 2) {
                         const float la = fmaf((float)z, dlv, lv0), lb = fmaf((float)(z + 1), dlv, lv0);
@@ -277,6 +344,7 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
                         const bool up = fb.bits != fa.bits;
                         acc[z + 1] = fmaf(lerp_ref(up ? p1 : p0, up ? p2 : p1, fb.f), rw2, acc[z + 1]);
                     }
+#endif
                 } else {
 #pragma unroll
                     for (int z = 0; z < TB_Z; ++z) {
@@ -319,6 +387,16 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
             }
         }
     }
+    __syncthreads();
+    if (tid == 0 && s_failed < n_pass) {
+        // boxes possibly still in flight: those of the pass waited for in
+        // vain and of the pass issued before that wait; the CTA must not
+        // exit while they can still write its shared memory
+        const int q = s_failed;
+        for (int r = q; r <= q + 1 && r < n_pass; ++r)
+            mbar_wait_bounded(&full[r & 1], (r >> 1) & 1, nullptr, PYRONN_BP_SPINS);
+    }
+#undef PYRONN_BP_SPINS
     if (i < X && j < Y) {
         const float mv = mult[g];
         Tout *vol_b = vol + (size_t)b * Z * Y * X;
@@ -367,7 +445,7 @@ CUtensorMapDataType tma_type<__half>()
 
 template <typename Tin, typename Tout>
 cudaError_t launch_typed(const void *sinogram, void *volume, const Dims3D &d, const ConeBpView *views,
-                         const float *mult, unsigned *err, cudaStream_t stream)
+                         const float *mult, unsigned *err, int starve_last_pass, cudaStream_t stream)
 {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return cudaErrorNotSupported;
@@ -384,7 +462,7 @@ cudaError_t launch_typed(const void *sinogram, void *volume, const Dims3D &d, co
     const dim3 block(TB_X, TB_Y, 1);
     const dim3 grid((d.vol_x + TB_X - 1) / TB_X, (d.vol_y + TB_Y - 1) / TB_Y, zblocks * d.batch);
     static_assert((BOX_ELEMS * sizeof(float)) % 128 == 0 && (BOX_ELEMS * 2) % 128 == 0, "tile alignment");
-    const size_t smem = 2 * BP_K * BOX_ELEMS * sizeof(Tin) + 128;
+    const size_t smem = 2 * BpViews<Tin>::K * BOX_ELEMS * sizeof(Tin) + 128;
     // set on every launch: the attribute belongs to the current device's copy
     // of the kernel, and the call is a cheap host-side update
     cudaError_t e = cudaFuncSetAttribute(cone_bp_tma_kernel<Tin, Tout>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -392,7 +470,7 @@ cudaError_t launch_typed(const void *sinogram, void *volume, const Dims3D &d, co
     if (e != cudaSuccess) return e;
     cone_bp_tma_kernel<Tin, Tout><<<grid, block, smem, stream>>>(map, (const Tin *)sinogram, (Tout *)volume, views, mult,
                                                                d.vol_x, d.vol_y, d.vol_z, d.det_w, d.det_h, d.n_proj,
-                                                               d.geom_batch, err);
+                                                               d.geom_batch, err, starve_last_pass);
     return cudaGetLastError();
 }
 
@@ -411,13 +489,23 @@ bool cone_bp_tma_supported(const void *sinogram, int in_dtype, const Dims3D &d)
     return encode_fn() != nullptr;
 }
 
+namespace {
+std::atomic<int> g_starve_last_pass{0};
+}  // namespace
+
+void cone_bp_tma_starve_last_pass(int enable)
+{
+    g_starve_last_pass.store(enable ? 1 : 0);
+}
+
 cudaError_t launch_cone_bp_tma(const void *sinogram, void *volume, int in_dtype, int out_dtype, const Dims3D &d,
                                const ConeBpView *views, const float *mult, unsigned *err, cudaStream_t stream)
 {
+    const int starve = g_starve_last_pass.load();
     return dispatch_dtypes(in_dtype, out_dtype, [&](auto tin, auto tout) {
         using Tin = typename decltype(tin)::type;
         using Tout = typename decltype(tout)::type;
-        return launch_typed<Tin, Tout>(sinogram, volume, d, views, mult, err, stream);
+        return launch_typed<Tin, Tout>(sinogram, volume, d, views, mult, err, starve, stream);
     });
 }
 

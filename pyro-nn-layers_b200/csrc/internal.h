@@ -76,6 +76,9 @@ bool fdk_tc_supported(long long rows, int W, const void *in, const void *out);
 cudaError_t launch_fdk_filter_tc(const void *in, void *out, int in_dtype, int out_dtype, long long rows, int det_h,
                                  int W, float sdd, float dv, float du, float cv, float cu, int kind,
                                  int weight_output, cudaStream_t stream);
+// reads the filter's sticky device error word on the current device (and
+// clears it when set); synchronises the stream
+cudaError_t fdk_tc_error(cudaStream_t stream, unsigned *device_error);
 
 cudaError_t launch_cone_scatter(const void *sinogram, float *volume, int in_dtype, const Dims3D &d,
                                 const ConeFpView *views, const float *step, const float *spacing,
@@ -85,6 +88,10 @@ cudaError_t launch_cone_scatter(const void *sinogram, float *volume, int in_dtyp
 bool cone_bp_tma_supported(const void *sinogram, int in_dtype, const Dims3D &d);
 cudaError_t launch_cone_bp_tma(const void *sinogram, void *volume, int in_dtype, int out_dtype, const Dims3D &d,
                                const ConeBpView *views, const float *mult, unsigned *err, cudaStream_t stream);
+// testing hook (pyronn_debug_starve_tma_wait): while enabled, the last pass of
+// every TMA backprojector block issues no copies and expects bytes that never
+// arrive, so its bounded wait runs out and the block reports the timeout
+void cone_bp_tma_starve_last_pass(int enable);
 
 // texture-array cache (texcache.cu)
 struct CachedArray;

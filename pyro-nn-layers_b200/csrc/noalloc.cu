@@ -10,6 +10,10 @@
 // the library image itself provides: it exists on every GPU that loads the
 // library, from load until process exit, and no call ever allocates.
 //
+// The first word of the scratch is the call's device error flag (cleared at
+// the start of every call, set when a bounded wait of the TMA backprojector
+// gives up); pyronn_noalloc_error reads it without a workspace pointer.
+//
 // Limits: geom_batch * n_proj <= PYRONN_NOALLOC_MAX_VIEWS (bigger requests
 // are rejected); software interpolation only (hardware_interp needs CUDA
 // arrays, which are allocations).  Every call on a device shares the one
@@ -83,4 +87,20 @@ extern "C" int pyronn_cone_backprojection3d_noalloc(const void *sinogram, void *
     return pyronn_cone_backprojection3d(sinogram, volume, in_dtype, out_dtype, 0, batch, n_proj, det_h, det_w, vol_z,
                                         vol_y, vol_x, volume_origin, volume_spacing, projection_matrices, step_size,
                                         projection_multiplier, geom_batch, scratch, bytes, stream);
+}
+
+extern "C" int pyronn_noalloc_error(void *stream, int *device_error)
+{
+    if (!device_error) return report_error(PYRONN_ERROR_INVALID_ARGUMENT, "noalloc_error: null pointer");
+    void *scratch = nullptr;
+    cudaError_t e = scratch_address(&scratch);
+    if (e != cudaSuccess) return report_cuda_error(e, "noalloc_error: scratch address");
+    // the header word (a pageable host copy: synchronous for the host)
+    unsigned flag = 0;
+    cudaStream_t s = (cudaStream_t)stream;
+    e = cudaMemcpyAsync(&flag, scratch, sizeof(flag), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return report_cuda_error(e, "noalloc_error");
+    *device_error = (int)flag;
+    return report_error(PYRONN_SUCCESS, "%s", "");
 }

@@ -230,16 +230,24 @@ __global__ void __launch_bounds__(FP2_BLOCK, 12)
     const float ox = geo.volume_origin[2 * g + 1], oy = geo.volume_origin[2 * g + 0];
     const float ds = geo.detector_spacing[g], dorg = geo.detector_origin[g];
     const float2 ray_in = reinterpret_cast<const float2 *>(geo.rays)[(size_t)g * n_proj + p];
-    const float uu = (float)u * ds + dorg;
+    const float uu = __fmaf_rn((float)u, ds, dorg);  // index_to_physical, helper_grid.h
 
     double srcx, srcy, rx, ry;
     if (!FAN) {
-        // par_projector_2D_CudaKernel.cu.cc:120-132
-        const float sid = sqrtf((float)((float)X * sx * (float)X * sx) + ((float)Y * sy * (float)Y * sy)) * 1.2f;
+        // par_projector_2D_CudaKernel.cu.cc:120-132.  The virtual source point
+        // is formed in FP32 as the reference forms it (ray * (-sid) + u_vec *
+        // u, the second product fused) before the FP64 box test: a ray that
+        // grazes the box -- along an axis with a 1e-17 cross component, say
+        // -- enters or misses on that rounding, as in the reference.
+        const float fx = (float)X, fy = (float)Y;
+        const float sid =
+            __fmul_rn(sqrtf(__fadd_rn(__fmul_rn(__fmul_rn(__fmul_rn(fx, sx), fx), sx),
+                                      __fmul_rn(__fmul_rn(__fmul_rn(fy, sy), fy), sy))),
+                      1.2f);
         rx = ray_in.x;
         ry = ray_in.y;
-        srcx = (double)ray_in.x * -(double)sid + (double)(-ray_in.y) * (double)uu;
-        srcy = (double)ray_in.y * -(double)sid + (double)ray_in.x * (double)uu;
+        srcx = (double)__fmaf_rn(-ray_in.y, uu, __fmul_rn(ray_in.x, -sid));
+        srcy = (double)__fmaf_rn(ray_in.x, uu, __fmul_rn(ray_in.y, -sid));
     } else {
         // fan_projector_2D_CudaKernel.cu.cc:122-133
         const double sid = geo.sid[g], sdd = geo.sdd[g];
@@ -329,6 +337,34 @@ struct RowTaps<float> {
     }
 };
 
+// Detector index of pixel c for one fan view by the reference's own FP32
+// steps: source r * (-SID), central point source + r * SDD, intersectLines2D
+// (pixel, source, centre, centre + (-r.y, r.x)) and physical_to_index
+// (fan_backprojector_2D_CudaKernel.cu.cc:47-59, helper_geometry_gpu.h:28-44),
+// each operation rounded once.  Used for pixels near the source's depth,
+// where the lines are nearly parallel and the reference's FP32 intersection
+// differs from the exact one: its denominator below 1e-6 gives NaN, which the
+// texture unit samples as coordinate 0 (measured on B200: half of the view's
+// first texel, i.e. index -0.5); just above it, a far-off point.
+__device__ __noinline__ float fan_index_reference_steps(float cx, float cy, float rx, float ry, float sid, float sdd,
+                                                        float dorg, float ds)
+{
+    const float srcx = __fmul_rn(rx, -sid), srcy = __fmul_rn(ry, -sid);
+    const float cpx = __fadd_rn(srcx, __fmul_rn(rx, sdd)), cpy = __fadd_rn(srcy, __fmul_rn(ry, sdd));
+    const float detx = -ry, dety = rx;
+    const float p4x = __fadd_rn(cpx, detx), p4y = __fadd_rn(cpy, dety);
+    const float a1 = __fsub_rn(cx, srcx), b1 = __fsub_rn(cpy, p4y);
+    const float a2 = __fsub_rn(cy, srcy), b2 = __fsub_rn(cpx, p4x);
+    const float dn = __fsub_rn(__fmul_rn(a1, b1), __fmul_rn(a2, b2));
+    if (dn < 1.0e-6f && dn > -1.0e-6f) return -0.5f;
+    const float x12 = __fsub_rn(__fmul_rn(cx, srcy), __fmul_rn(cy, srcx));
+    const float x34 = __fsub_rn(__fmul_rn(cpx, p4y), __fmul_rn(cpy, p4x));
+    const float x = __fdiv_rn(__fsub_rn(__fmul_rn(x12, b2), __fmul_rn(a1, x34)), dn);
+    const float y = __fdiv_rn(__fsub_rn(__fmul_rn(x12, b1), __fmul_rn(a2, x34)), dn);
+    const float s = __fadd_rn(__fmul_rn(x, detx), __fmul_rn(y, dety));
+    return __fdiv_rn(__fsub_rn(s, dorg), ds);
+}
+
 // One thread per pixel, views in chunks of BP2_CHUNK whose per-view
 // constants the block first puts in shared memory (one view per thread):
 // parallel beam (-r.y, r.x) / detector spacing, fan beam (r.x, r.y, SID |r|^2,
@@ -387,7 +423,11 @@ __global__ void __launch_bounds__(BP2_BLOCK_X *BP2_BLOCK_Y)
                 // s = SDD |r|^2 <c, d> / (<c, r> + SID |r|^2), weight 1 / |c - src|^2
                 const float cd = fmaf(cy, q.x, -cx * q.y);
                 const float cr = fmaf(cx, q.x, cy * q.y);
-                sidx = fmaf(q.w * cd, fast_rcp(cr + q.z), -sdo);
+                const float den = cr + q.z;  // <c - src, r>: the pixel's depth from the source
+                sidx = fmaf(q.w * cd, fast_rcp(den), -sdo);
+                // within 1e-2 mm of the source's depth, the reference's FP32
+                // steps decide (rare: the source inside or at the field)
+                if (fabsf(den) < 1.0e-2f) sidx = fan_index_reference_steps(cx, cy, q.x, q.y, sid, sdd, dorg, ds);
                 const float ex = fmaf(q.x, sid, cx), ey = fmaf(q.y, sid, cy);
                 w = fast_rcp(fmaf(ex, ex, ey * ey));
             }

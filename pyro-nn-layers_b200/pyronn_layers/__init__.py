@@ -11,18 +11,21 @@ They run hand-written sm_100a CUDA kernels through the C ABI of
 ``include/pyronn_b200.h`` (``libpyronn_b200.so`` in this directory).
 """
 from .ops import (  # noqa: F401
+    check_device_errors,
     circular_projection_matrices,
     circular_ray_vectors_2d,
     cone_backprojection3d,
     cone_backprojection3d_matched,
     cone_projection3d,
+    device_errors,
     fan_backprojection2d,
     fan_projection2d,
     parallel_backprojection2d,
     parallel_projection2d,
     release_cached_arrays,
+    set_sync_error_checks,
 )
-from ._capi import PyronnError  # noqa: F401
+from ._capi import PyronnDeviceError, PyronnError  # noqa: F401
 from . import fbp, geometry, phantoms  # noqa: F401
 
 __all__ = [
@@ -37,6 +40,10 @@ __all__ = [
     "circular_projection_matrices",
     "circular_ray_vectors_2d",
     "PyronnError",
+    "PyronnDeviceError",
+    "check_device_errors",
+    "device_errors",
+    "set_sync_error_checks",
     "fbp",
     "geometry",
     "phantoms",

@@ -36,6 +36,9 @@ PROTOTYPES = {
     "pyronn_last_error": (ctypes.c_char_p, []),
     "pyronn_release_cached_arrays": (_I, []),
     "pyronn_workspace_error": (_I, [_P, _P, _P]),
+    "pyronn_debug_starve_tma_wait": (_I, [_I]),
+    "pyronn_noalloc_error": (_I, [_P, _P]),
+    "pyronn_fdk_error": (_I, [_P, _P]),
     "pyronn_projection2d_workspace_size": (_SZ, [_I] * 4),
     "pyronn_parallel_projection2d": (
         _I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _P, _SZ, _P]),
@@ -59,6 +62,9 @@ PROTOTYPES = {
     "pyronn_fdk_filter": (_I, [_P, _P, _I, _I, _I, _I, _I, _I] + [_D] * 5 + [_I, _I, _P]),
 }
 
+DEVICE_ERROR_NONE = 0  # PYRONN_DEVICE_ERROR_NONE
+DEVICE_ERROR_WAIT_TIMEOUT = 1  # PYRONN_DEVICE_ERROR_WAIT_TIMEOUT
+
 NOALLOC_MAX_VIEWS = 8192  # PYRONN_NOALLOC_MAX_VIEWS
 FILTER_RAM_LAK = 0  # PYRONN_FILTER_RAM_LAK
 FILTER_SHEPP_LOGAN = 1  # PYRONN_FILTER_SHEPP_LOGAN
@@ -74,6 +80,16 @@ class PyronnError(RuntimeError):
         self.detail = detail
         super().__init__("%s failed: %s (status %d)%s" % (
             func, _status_name(status), status, (": " + detail) if detail else ""))
+
+
+class PyronnDeviceError(RuntimeError):
+    """A kernel reported a device-side failure (a bounded wait that gave up)
+    after its call had returned: the affected results were not written."""
+
+    def __init__(self, flags, what="device"):
+        self.flags = flags
+        super().__init__("%s error flags 0x%x: a bounded wait for an asynchronous copy or tensor-core "
+                         "operation gave up; the affected output was not written" % (what, flags))
 
 
 def _status_name(status):

@@ -43,6 +43,8 @@ def _run_filter(x: torch.Tensor, params, weight_output: bool, out_dtype) -> torc
         _capi.call("pyronn_fdk_filter", x4.data_ptr(), out.data_ptr(), ops.storage_code(x4.dtype),
                    ops.storage_code(od), b, n, h, w, sdd, dv, du, cv, cu, code, int(weight_output),
                    ops._stream(x.device))
+        if ops._sync_error_checks:  # otherwise ops.device_errors() reads the filter's word
+            ops.check_device_errors(x.device)
     return out if x.dim() == 4 else out.squeeze(2)
 
 

@@ -19,11 +19,20 @@ mirrors ``REGISTER_OP("ConeProjection3D")`` (cc/ops/cone_projector_3D_OPKernel.c
   vice versa (the pairing the PYRO-NN package registers for these ops); the
   geometry inputs get no gradient.
 * Errors raise :class:`~pyronn_layers._capi.PyronnError` (the reference exits
-  the process or ignores CUDA errors).
+  the process or ignores CUDA errors).  Kernels with bounded device-side waits
+  (the TMA-staged cone backprojector, the tensor-core FDK filter) report a
+  wait that gave up through a device flag after the call has returned: the
+  ops fold those flags into a per-device word on the stream, without
+  synchronising, and :func:`check_device_errors` (or ``device_errors``) reads
+  it at a point where the caller synchronises anyway;
+  ``set_sync_error_checks(True)`` or ``PYRONN_SYNC_ERROR_CHECKS=1`` makes
+  every such op synchronise and raise at once instead.
 """
 from __future__ import annotations
 
+import ctypes
 import math
+import os
 from typing import Sequence
 
 import torch
@@ -93,6 +102,76 @@ def _check_data(x: torch.Tensor, ndim: int, what: str):
 
 def _stream(device) -> int:
     return torch.cuda.current_stream(device).cuda_stream
+
+
+# ------------------------------------------------------------ device error flags
+
+_sync_error_checks = os.environ.get("PYRONN_SYNC_ERROR_CHECKS", "0") not in ("", "0")
+_error_words = {}  # device index -> int32 [1]: OR of the device error flags seen
+
+
+def set_sync_error_checks(enabled: bool) -> None:
+    """With True, every op with bounded device-side waits synchronises after
+    its launch and raises PyronnDeviceError if a wait gave up (debugging);
+    with False (the default) the flags accumulate on the device for
+    check_device_errors."""
+    global _sync_error_checks
+    _sync_error_checks = bool(enabled)
+
+
+def _error_word(device):
+    idx = device.index if device.index is not None else torch.cuda.current_device()
+    w = _error_words.get(idx)
+    if w is None:
+        if torch.cuda.is_current_stream_capturing():
+            return None  # created outside captures only (a capture's pool may be freed with its graph)
+        w = torch.zeros(1, dtype=torch.int32, device=torch.device("cuda", idx))
+        _error_words[idx] = w
+    return w
+
+
+def note_workspace_error(workspace: torch.Tensor, device) -> None:
+    """Folds the device error flag that the call just enqueued on the current
+    stream leaves in its workspace header (first 32-bit word) into the
+    device's error word, on that stream (no synchronisation)."""
+    flag = workspace[:4].view(torch.int32)
+    if _sync_error_checks and not torch.cuda.is_current_stream_capturing():
+        value = int(flag.item())
+        if value:
+            raise _capi.PyronnDeviceError(value, "cone backprojection")
+        return
+    w = _error_word(device)
+    if w is not None:
+        w.bitwise_or_(flag)
+
+
+def device_errors(device=None, clear: bool = True) -> int:
+    """Synchronises the device and returns the OR of the device error flags
+    raised since the last call (pyronn_layers ops' workspaces and the
+    tensor-core FDK filter's word): 0 when every bounded wait completed,
+    _capi.DEVICE_ERROR_WAIT_TIMEOUT when one gave up and its output was not
+    written."""
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    if dev.index is None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+    torch.cuda.synchronize(dev)
+    value = 0
+    w = _error_words.get(dev.index)
+    if w is not None:
+        value = int(w.item())
+        if clear:
+            w.zero_()
+    flag = ctypes.c_int(0)
+    with torch.cuda.device(dev):
+        _capi.call("pyronn_fdk_error", _stream(dev), ctypes.byref(flag))
+    return value | flag.value
+
+
+def check_device_errors(device=None) -> None:
+    """Raises PyronnDeviceError if device_errors() reports a flag."""
+    value = device_errors(device)
+    if value:
+        raise _capi.PyronnDeviceError(value)
 
 
 # ---------------------------------------------------------------- geometry packs
@@ -223,6 +302,8 @@ def _run_cone(forward: bool, x: torch.Tensor, out_dims, geo: GeometryCone, hardw
         _capi.call(fn, x.data_ptr(), out.data_ptr(), storage_code(x.dtype), storage_code(od),
                    int(bool(hardware_interp)), *dims, *geo.pointers(), geo.g, workspace.data_ptr(),
                    workspace.numel(), _stream(dev))
+        if not forward and not hardware_interp:
+            note_workspace_error(workspace, dev)  # the TMA-staged path's bounded waits
     return out
 
 

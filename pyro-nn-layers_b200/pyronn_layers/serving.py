@@ -273,6 +273,9 @@ class Executor:
                 self._capi.call("pyronn_cone_backprojection3d", inp.data_ptr(), out.data_ptr(), code_in, code_out, 0,
                                 batch, n_proj, dh, dw, vz, vy, vx, *self.geo.pointers(), 1, ws.data_ptr(),
                                 ws.numel(), stream_handle)
+                # the batch's device error flag into the device's error word
+                # (on the batch's stream; captured with the launch)
+                self.ops.note_workspace_error(ws, self.device)
 
     def run(self, batch: int, bset: int, stream) -> None:
         """Enqueues the batch's kernels on stream (eager for the first runs,
@@ -500,6 +503,9 @@ class ProjectorServer:
                     time.sleep(min(wait, 0.001))
         torch.cuda.synchronize(self.device)
         wall = now()
+        # a bounded device wait that gave up leaves some result invalid
+        from . import ops
+        ops.check_device_errors(self.device)
         lat = np.array([(j.done - j.arrival) * 1e3 for j in jobs])
         replays = sum(ex.graph_replays for ex in self.executors.values())
         return ServeStats(lat, percentile(lat, 50), percentile(lat, 99), total_updates / wall / 1e9, wall,

@@ -1,6 +1,6 @@
 """Generates the golden fixtures tests/golden/*.npz from the reference itself.
 
-    python tests/golden/make_golden.py [--out DIR]     (needs a CUDA GPU)
+    python tests/golden/make_golden.py [--out DIR] [--only NAME,...]     (needs a CUDA GPU)
 
 Runs the reference's own CUDA launchers (cc/kernels/*.cu.cc of PYRO-NN-Layers,
 compiled unmodified into oracle/_ref/libpyronn_ref.so by oracle.build_ref(),
@@ -124,6 +124,36 @@ def case_fan(L):
                         sinogram_in=sino_in, volume_ref=vol_out.cpu().numpy().reshape(B, Y, X))
 
 
+def case_fan_degenerate(L):
+    """Fan backprojection with pixels on intersectLines2D's degenerate line:
+    the source inside the field (SID 5.5 mm, then 15.5 mm: the column of
+    pixels at x = -SID for the view along +x, and the row, column or row at
+    distance SID for the other axis views), where the reference's lines are
+    parallel and its intersection is NaN
+    (cc/helper_headers/helper_geometry_gpu.h:30-36)."""
+    B, Y, X, W = 2, 32, 32, 40
+    vs = np.array([[1.0, 1.0], [1.0, 1.0]], np.float32)
+    check_geometry(vs)
+    vo = np.stack([geometry.centered_origin((Y, X), vs[b]) for b in range(B)])
+    ds = np.array([[1.0], [1.0]], np.float32)
+    do = np.stack([geometry.detector_origin_1d(W, 1.0)] * B)
+    sid = np.array([[5.5], [15.5]], np.float32)
+    sdd = sid + np.float32(30.0)
+    views = np.array([[1.0, 0.0], [0.0, 1.0], [-1.0, 0.0], [0.0, -1.0], [0.6, 0.8],
+                      [math.cos(1.0), math.sin(1.0)]], np.float32)
+    rays = np.stack([views, views])
+    n_proj = views.shape[0]
+    rng = np.random.Generator(np.random.PCG64(9))
+    sino_in = rng.uniform(0.5, 1.0, (B, n_proj, W)).astype(np.float32)
+    vol_out = torch.zeros(B * Y * X, device="cuda")
+    check(L.ref_fan_backprojection2d(ptr(dev(sino_in)), ptr(vol_out), B, n_proj, W, Y, X, ptr(dev(vo)),
+                                     ptr(dev(do)), ptr(dev(vs)), ptr(dev(ds)), ptr(dev(sid)), ptr(dev(sdd)),
+                                     ptr(dev(rays))), "fan bp degenerate")
+    np.savez_compressed(os.path.join(OUT, "fan2d_degenerate.npz"), volume_shape=[Y, X], volume_origin=vo,
+                        volume_spacing=vs, detector_origin=do, detector_spacing=ds, sid=sid, sdd=sdd,
+                        ray_vectors=rays, sinogram_in=sino_in, volume_ref=vol_out.cpu().numpy().reshape(B, Y, X))
+
+
 def cone_case(L, name, vol_shape, spacing, det_shape, det_spacing, n_proj, sid, sdd, step, seed):
     Z, Y, X = vol_shape
     H, W = det_shape
@@ -157,21 +187,27 @@ def cone_case(L, name, vol_shape, spacing, det_shape, det_spacing, n_proj, sid, 
 
 def main():
     global OUT
-    if len(sys.argv) > 2 and sys.argv[1] == "--out":
-        OUT = sys.argv[2]
+    if "--out" in sys.argv:
+        OUT = sys.argv[sys.argv.index("--out") + 1]
         os.makedirs(OUT, exist_ok=True)
     L = load_ref()
     for f in ("ref_parallel_projection2d", "ref_parallel_backprojection2d", "ref_fan_projection2d",
               "ref_fan_backprojection2d", "ref_cone_projection3d", "ref_cone_backprojection3d"):
         getattr(L, f).restype = ctypes.c_int
     torch.cuda.init()
-    case_parallel(L)
-    case_fan(L)
-    # detector covers the whole volume shadow
-    cone_case(L, "cone3d", (24, 32, 40), (1.0, 1.0, 1.0), (40, 56), (1.5, 1.5), 24, 200.0, 320.0, 0.5, 30)
-    # small detector: the shadow overflows every edge (out-of-detector taps,
-    # the software backprojector's next-row / next-view taps)
-    cone_case(L, "cone3d_edges", (20, 28, 28), (1.0, 1.0, 1.0), (16, 20), (1.5, 1.5), 12, 150.0, 260.0, 0.7, 40)
+    only = sys.argv[sys.argv.index("--only") + 1].split(",") if "--only" in sys.argv else None
+    cases = {"parallel2d": lambda: case_parallel(L), "fan2d": lambda: case_fan(L),
+             "fan2d_degenerate": lambda: case_fan_degenerate(L),
+             # detector covers the whole volume shadow
+             "cone3d": lambda: cone_case(L, "cone3d", (24, 32, 40), (1.0, 1.0, 1.0), (40, 56), (1.5, 1.5), 24, 200.0,
+                                         320.0, 0.5, 30),
+             # small detector: the shadow overflows every edge (out-of-detector
+             # taps, the software backprojector's next-row / next-view taps)
+             "cone3d_edges": lambda: cone_case(L, "cone3d_edges", (20, 28, 28), (1.0, 1.0, 1.0), (16, 20), (1.5, 1.5),
+                                               12, 150.0, 260.0, 0.7, 40)}
+    for name, run in cases.items():
+        if only is None or name in only:
+            run()
     print("golden fixtures written to", OUT)
 
 

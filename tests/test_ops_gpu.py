@@ -6,10 +6,17 @@ Tolerances (relative L2):
   * FP32 arithmetic vs the FP64 oracle on the same (storage-rounded) input:
     2e-5 for ray marches (thousands of FP32 sums), 1e-5 for backprojections;
   * hardware_interp (texture unit, 8-bit interpolation weights) vs exact
-    weights: 5e-3;
+    weights: forward 5e-4 (measured 3.6e-5 to 6.7e-5), backprojection of a
+    noise sinogram 2e-3 (one texture-weighted fetch per update: the reference's
+    own outputs are 3.5e-4 to 6.0e-4 from the exact weights); 5e-3 on the
+    one-voxel and ragged shapes, where a handful of texels dominate;
   * 16-bit OUTPUT storage adds its rounding: 4e-3 (bf16), 6e-4 (fp16);
-  * against the reference's outputs: 1e-5 on the software cone paths, 5e-3
-    where the reference used texture weights (all 2D ops, hardware_interp).
+  * against the reference's outputs (golden fixtures): 1e-5 on the software
+    cone paths (measured below 6e-7); hardware_interp cone 5e-5 (the same
+    texture unit on both sides: measured 4.4e-6 to 1.9e-5); 2D forward 5e-5
+    (the reference's texture weights averaged over its 0.2 mm steps: measured
+    1.1e-5); 2D backprojection 5e-4 (one texture-weighted tap pair per view:
+    measured 1.1e-4 to 1.2e-4).
 """
 import ctypes
 import math
@@ -150,7 +157,7 @@ def test_cone_projection_vs_oracle(cuda, dtype, hw):
     x = t(vol, cuda, dtype)
     out = pl.cone_projection3d(x, geo.detector_shape, *geo.args(), hardware_interp=hw, out_dtype=torch.float32)
     ref = oracle.cone_projection3d(rounded(x), geo.detector_shape, *geo.args(), hardware_interp=hw)
-    tol = 5e-3 if hw else 2e-5
+    tol = 5e-4 if hw else 2e-5
     assert rel_l2(out.cpu().numpy(), ref) < tol
 
 
@@ -177,7 +184,7 @@ def test_cone_backprojection_vs_oracle(cuda, dtype, hw):
     p = t(rng.uniform(0, 1, (2,) + geo.detector_shape), cuda, dtype)
     out = pl.cone_backprojection3d(p, geo.volume_shape, *geo.args(), hardware_interp=hw, out_dtype=torch.float32)
     ref = oracle.cone_backprojection3d(rounded(p), geo.volume_shape, *geo.args(), hardware_interp=hw)
-    tol = 5e-3 if hw else 1e-5
+    tol = 2e-3 if hw else 1e-5  # one texture-weighted fetch per update on a noise sinogram
     assert rel_l2(out.cpu().numpy(), ref) < tol
     out16 = pl.cone_backprojection3d(p, geo.volume_shape, *geo.args(), hardware_interp=hw)
     assert rel_l2(out16.float().cpu().numpy(), ref) < tol + OUT_TOL[dtype]
@@ -254,9 +261,9 @@ def test_golden_parallel(cuda):
     g = load_golden("parallel2d")
     args = (g["volume_origin"], g["detector_origin"], g["volume_spacing"], g["detector_spacing"], g["ray_vectors"])
     out = pl.parallel_projection2d(t(g["volume"], cuda), g["projection_shape"], *args)
-    assert rel_l2(out.cpu().numpy(), g["sinogram_ref"]) < 5e-3
+    assert rel_l2(out.cpu().numpy(), g["sinogram_ref"]) < 5e-5
     out = pl.parallel_backprojection2d(t(g["sinogram_in"], cuda), g["volume"].shape[1:], *args)
-    assert rel_l2(out.cpu().numpy(), g["volume_ref"]) < 5e-3
+    assert rel_l2(out.cpu().numpy(), g["volume_ref"]) < 5e-4
 
 
 def test_golden_fan(cuda):
@@ -264,9 +271,34 @@ def test_golden_fan(cuda):
     args = (g["volume_origin"], g["detector_origin"], g["volume_spacing"], g["detector_spacing"], g["sid"], g["sdd"],
             g["ray_vectors"])
     out = pl.fan_projection2d(t(g["volume"], cuda), g["projection_shape"], *args)
-    assert rel_l2(out.cpu().numpy(), g["sinogram_ref"]) < 5e-3
+    assert rel_l2(out.cpu().numpy(), g["sinogram_ref"]) < 5e-5
     out = pl.fan_backprojection2d(t(g["sinogram_in"], cuda), g["volume"].shape[1:], *args)
-    assert rel_l2(out.cpu().numpy(), g["volume_ref"]) < 5e-3
+    assert rel_l2(out.cpu().numpy(), g["volume_ref"]) < 5e-4
+
+
+def test_golden_fan_degenerate_line(cuda):
+    """Pixels on and near intersectLines2D's degenerate line (the source
+    inside the field; cc/helper_headers/helper_geometry_gpu.h:30-36): the
+    reference's NaN intersection reaches its texture as a NaN coordinate,
+    which samples as coordinate 0 -- half of the view's first texel -- and
+    just off the line its FP32 intersection lands far from the exact one; the
+    kernel takes the reference's FP32 steps within 1e-2 mm of the source's
+    depth.  Matched against the reference's own outputs (golden fixture) and
+    the oracle, which follows the same rule."""
+    g = load_golden("fan2d_degenerate")
+    args = (g["volume_origin"], g["detector_origin"], g["volume_spacing"], g["detector_spacing"], g["sid"], g["sdd"],
+            g["ray_vectors"])
+    out = pl.fan_backprojection2d(t(g["sinogram_in"], cuda), tuple(g["volume_shape"]), *args).cpu().numpy()
+    ref = g["volume_ref"]
+    assert np.isfinite(out).all()
+    assert rel_l2(out, ref) < 5e-4
+    # the column of pixels at x = -SID for the view along +x (batch 0: SID 5.5,
+    # column 10; batch 1: SID 15.5, column 0) carries the degenerate taps
+    for b, col in ((0, 10), (1, 0)):
+        np.testing.assert_allclose(out[b, :, col], ref[b, :, col], rtol=1e-3, atol=1e-3 * np.abs(ref[b, :, col]).max())
+    # and the FP64 oracle follows the same rule
+    orc = oracle.fan_backprojection2d(g["sinogram_in"], tuple(g["volume_shape"]), *args)
+    assert rel_l2(out, orc) < 1e-5
 
 
 @pytest.mark.parametrize("name", ["cone3d", "cone3d_edges"])
@@ -275,7 +307,7 @@ def test_golden_cone(cuda, name, hw):
     g = load_golden(name)
     args = (g["volume_origin"], g["volume_spacing"], g["projection_matrices"], g["step_size"],
             g["projection_multiplier"])
-    tol = 5e-3 if hw else 1e-5
+    tol = 5e-5 if hw else 1e-5
     out = pl.cone_projection3d(t(g["volume"], cuda), g["projection_shape"], *args, hardware_interp=bool(hw))
     assert rel_l2(out.cpu().numpy(), g["sinogram_ref_hw%d" % hw]) < tol
     out = pl.cone_backprojection3d(t(g["sinogram_in"], cuda), g["volume"].shape[1:], *args,

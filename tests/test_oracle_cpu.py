@@ -98,10 +98,12 @@ def test_fan_backprojection_closed_form_matches_intersection():
 def test_oracle_matches_reference_parallel():
     g = load_golden("parallel2d")
     args = (g["volume_origin"], g["detector_origin"], g["volume_spacing"], g["detector_spacing"], g["ray_vectors"])
+    # the reference samples with 8-bit texture weights: measured 1.1e-5 (its
+    # forward averages them over 0.2 mm steps) and 1.2e-4 (one tap pair per view)
     sino = oracle.parallel_projection2d(g["volume"], g["projection_shape"], *args)
-    assert rel_l2(sino, g["sinogram_ref"]) < 5e-3  # reference: 8-bit texture weights
+    assert rel_l2(sino, g["sinogram_ref"]) < 5e-5
     vol = oracle.parallel_backprojection2d(g["sinogram_in"], g["volume"].shape[1:], *args)
-    assert rel_l2(vol, g["volume_ref"]) < 5e-3
+    assert rel_l2(vol, g["volume_ref"]) < 5e-4
 
 
 def test_oracle_matches_reference_fan():
@@ -109,9 +111,9 @@ def test_oracle_matches_reference_fan():
     args = (g["volume_origin"], g["detector_origin"], g["volume_spacing"], g["detector_spacing"], g["sid"], g["sdd"],
             g["ray_vectors"])
     sino = oracle.fan_projection2d(g["volume"], g["projection_shape"], *args)
-    assert rel_l2(sino, g["sinogram_ref"]) < 5e-3
+    assert rel_l2(sino, g["sinogram_ref"]) < 5e-5  # measured 1.1e-5
     vol = oracle.fan_backprojection2d(g["sinogram_in"], g["volume"].shape[1:], *args)
-    assert rel_l2(vol, g["volume_ref"]) < 5e-3
+    assert rel_l2(vol, g["volume_ref"]) < 5e-4  # measured 1.1e-4
 
 
 @pytest.mark.parametrize("name", ["cone3d", "cone3d_edges"])
@@ -120,11 +122,12 @@ def test_oracle_matches_reference_cone(name, hw):
     g = load_golden(name)
     args = (g["volume_origin"], g["volume_spacing"], g["projection_matrices"], g["step_size"],
             g["projection_multiplier"])
-    tol = 5e-3 if hw else 1e-5
+    # hardware_interp: exact weights here, 8-bit texture weights in the
+    # reference: measured 5.1e-5 / 5.3e-5 (forward), 3.5e-4 / 6.0e-4 (back)
     sino = oracle.cone_projection3d(g["volume"], g["projection_shape"], *args, hardware_interp=hw)
-    assert rel_l2(sino, g["sinogram_ref_hw%d" % hw]) < tol
+    assert rel_l2(sino, g["sinogram_ref_hw%d" % hw]) < (2e-4 if hw else 1e-5)
     vol = oracle.cone_backprojection3d(g["sinogram_in"], g["volume"].shape[1:], *args, hardware_interp=hw)
-    assert rel_l2(vol, g["volume_ref_hw%d" % hw]) < tol
+    assert rel_l2(vol, g["volume_ref_hw%d" % hw]) < (2e-3 if hw else 1e-5)
 
 
 def test_matched_backprojection_is_the_transpose():
@@ -177,3 +180,18 @@ def test_oracle_fdk_reconstructs_ellipsoids():
     c = slice(12, 36)
     assert abs(rec[c, c, c].mean() / vol[c, c, c].mean() - 1) < 0.01
     assert np.linalg.norm(rec[c, c, c] - vol[c, c, c]) / np.linalg.norm(vol[c, c, c]) < 0.08
+
+
+def test_oracle_matches_reference_on_the_degenerate_fan_line():
+    """intersectLines2D's NaN (parallel lines: pixels at the source's depth)
+    reaches the reference's tex2D as a NaN coordinate, sampled as coordinate 0
+    (half of the view's first texel); the oracle follows that rule and matches
+    the reference's own outputs there."""
+    g = load_golden("fan2d_degenerate")
+    args = (g["volume_origin"], g["detector_origin"], g["volume_spacing"], g["detector_spacing"], g["sid"], g["sdd"],
+            g["ray_vectors"])
+    out = oracle.fan_backprojection2d(g["sinogram_in"], tuple(g["volume_shape"]), *args)
+    assert np.isfinite(out).all()
+    assert rel_l2(out, g["volume_ref"]) < 5e-4
+    col = g["volume_ref"][0, :, 10]
+    np.testing.assert_allclose(out[0, :, 10], col, rtol=1e-3, atol=1e-3 * np.abs(col).max())

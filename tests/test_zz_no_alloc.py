@@ -70,3 +70,28 @@ def test_no_alloc_refuses_more_views_than_its_scratch(cuda):
                                                       x.data_ptr(), 1, None)
     assert status == _capi.ERROR_UNSUPPORTED
     assert b"exceeds the fixed scratch" in lib.pyronn_last_error()
+
+
+def test_no_alloc_reports_a_timed_out_wait(cuda):
+    """The entry point's device error flag sits in its fixed scratch, which
+    callers cannot address: pyronn_noalloc_error reads it.  The testing hook
+    pyronn_debug_starve_tma_wait makes the backprojector's bounded wait run
+    out (no copy in flight); the flag reports it, and the next call, unstarved,
+    clears it and gives the workspace entry point's result."""
+    import ctypes
+    geo, sino, gc = _case(cuda, 3, (16, 8, 32), (64, 64), 4, 1, torch.float32)
+    stream = torch.cuda.current_stream().cuda_stream
+    flag = ctypes.c_int(-1)
+    _capi.call("pyronn_debug_starve_tma_wait", 1)
+    try:
+        _no_alloc(geo, sino, gc)
+    finally:
+        _capi.call("pyronn_debug_starve_tma_wait", 0)
+    _capi.call("pyronn_noalloc_error", stream, ctypes.byref(flag))
+    assert flag.value == _capi.DEVICE_ERROR_WAIT_TIMEOUT
+    got = _no_alloc(geo, sino, gc)
+    _capi.call("pyronn_noalloc_error", stream, ctypes.byref(flag))
+    assert flag.value == _capi.DEVICE_ERROR_NONE
+    ref = _with_workspace(geo, sino, gc)
+    torch.cuda.synchronize()
+    assert rel_l2(got.cpu().numpy(), ref.cpu().numpy()) < 1e-5
