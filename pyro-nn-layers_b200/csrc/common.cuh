@@ -151,30 +151,6 @@ __device__ __forceinline__ FloorFrac floor_frac(float x)
     return r;
 }
 
-// floor_frac of the two halves of an f32x2 value with packed FP32
-// instructions (sm_100): the same three additions, each for both halves.
-struct FloorFrac2 {
-    int bits0, bits1;  // floor + FLOOR_BIAS of each half
-    float2 f;          // fractions
-};
-
-__device__ __forceinline__ FloorFrac2 floor_frac2(float2 x)
-{
-    const float2 y = __fadd2_rd(x, make_float2(12582912.0f, 12582912.0f));
-    const float2 fl = __fadd2_rn(y, make_float2(-12582912.0f, -12582912.0f));
-    FloorFrac2 r;
-    r.bits0 = __float_as_int(y.x);
-    r.bits1 = __float_as_int(y.y);
-    r.f = __ffma2_rn(fl, make_float2(-1.0f, -1.0f), x);  // x - floor(x), exact
-    return r;
-}
-
-// lerp_ref on both halves: fma(b, t, fma(a, -t, a)) per half
-__device__ __forceinline__ float2 lerp_ref2(float2 a, float2 b, float2 t, float2 neg_t)
-{
-    return __ffma2_rn(b, t, __ffma2_rn(a, neg_t, a));
-}
-
 // Approximate reciprocal (one MUFU op, <= 1 ulp).
 __device__ __forceinline__ float fast_rcp(float x)
 {

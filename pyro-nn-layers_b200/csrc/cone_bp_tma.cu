@@ -4,7 +4,7 @@
 //
 // Block = 256 threads = 32 (x) x 8 (y) voxels, each thread walks 16 voxels
 // along z: a 32 x 8 x 16 voxel tile.  Views are processed in passes of
-// BP_K views (BpViews).  For every view of a pass one warp (of four views) projects the 8 tile corners,
+// BP_K views.  For every view of a pass one warp projects the 8 tile corners,
 // takes the bounding box of the taps the tile can touch (+1 pixel margin), and
 // one thread issues a 3D TMA load of a BW x BH detector box around it into
 // shared memory; the next pass's boxes load while the current pass computes
@@ -43,25 +43,10 @@ namespace pyronn {
 
 namespace {
 
-#ifndef PYRONN_BP_PAIRS
-#define PYRONN_BP_PAIRS 0
-#endif
 constexpr int TB_X = 32;
 constexpr int TB_Y = 8;
 constexpr int TB_Z = 16;  // voxels per thread along z
-#ifndef PYRONN_BP_K16
-#define PYRONN_BP_K16 4
-#endif
-constexpr int BP_K_MAX = 8;
-// views per pass: 4 for FP32 sinograms, PYRONN_BP_K16 for 16-bit ones (two
-// stages of K boxes must leave room for 4 blocks per SM)
-template <typename T>
-struct BpViews {
-    static constexpr int K = sizeof(T) == 2 ? PYRONN_BP_K16 : 4;
-    // a warp sets up four views; the last warp's surplus lanes set up views of
-    // the next pass into unused meta slots, which nothing reads
-    static_assert(K % 2 == 0 && K >= 4 && K <= BP_K_MAX, "views per pass");
-};
+constexpr int BP_K = 4;  // views per pass
 constexpr int BOX_W = 72;  // 72-element rows shift banks between rows (64 would alias them)
 constexpr int BOX_H = 24;
 constexpr int BOX_ELEMS = BOX_W * BOX_H;
@@ -205,9 +190,8 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
     // TMA destinations must be 128-byte aligned: round the base up (the
     // launch reserves 128 spare bytes); every tile is a multiple of 128 bytes
     unsigned char *tile_base = dyn_smem + ((128u - (smem_addr(dyn_smem) & 127u)) & 127u);
-    constexpr int BP_K = BpViews<T>::K;
     T(*tiles)[BP_K][BOX_ELEMS] = reinterpret_cast<T(*)[BP_K][BOX_ELEMS]>(tile_base);  // [2][BP_K][BOX_ELEMS]
-    __shared__ __align__(16) ViewMeta meta[2][BP_K_MAX];
+    __shared__ __align__(16) ViewMeta meta[2][BP_K];
     __shared__ __align__(8) uint64_t full[2];
     __shared__ int s_failed;  // first pass whose wait gave up, n_pass if none (kept out of registers)
 
@@ -252,17 +236,9 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
                 tma_load_3d(&tiles[s][k][0], &tmap, meta[s][k].iu0, meta[s][k].iv0, b * n_proj + n, &full[s]);
         }
     };
-    // the warps that set up a pass's views (four each) meet before thread 0
-    // issues its loads
-    auto meta_ready = [&]() {
-        if (BP_K == 4)
-            __syncwarp();
-        else
-            asm volatile("bar.sync 1, %0;" ::"r"((BP_K + 3) / 4 * 32) : "memory");
-    };
-    if (warp < (BP_K + 3) / 4) {
-        pass_meta<T>(meta[0] + 4 * warp, pv, 4 * warp, n_proj, i0, j0, k0, W, H);
-        meta_ready();
+    if (warp == 0) {
+        pass_meta<T>(meta[0], pv, 0, n_proj, i0, j0, k0, W, H);
+        __syncwarp();
     }
     __syncthreads();
     if (tid == 0) issue(0, 0);
@@ -277,9 +253,9 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
     for (int p = 0; p < n_pass; ++p) {
         const int cur = p & 1, nxt = cur ^ 1;
         __syncthreads();  // pass p-1 is done with stage nxt
-        if (warp < (BP_K + 3) / 4 && p + 1 < n_pass) {
-            pass_meta<T>(meta[nxt] + 4 * warp, pv, (p + 1) * BP_K + 4 * warp, n_proj, i0, j0, k0, W, H);
-            meta_ready();
+        if (warp == 0 && p + 1 < n_pass) {
+            pass_meta<T>(meta[nxt], pv, (p + 1) * BP_K, n_proj, i0, j0, k0, W, H);
+            __syncwarp();
             if (tid == 0) issue(p + 1, nxt);
         }
         if (s_failed == n_pass && !mbar_wait_bounded(&full[cur], (p >> 1) & 1, err, PYRONN_BP_SPINS))
@@ -309,29 +285,6 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
                     // reads rows r, r + 1, r + 2 once (three u lerps for two
                     // voxels instead of four) and gives each voxel the same
                     // taps, hence the same bits, as the loop below
-#if PYRONN_BP_PAIRS
-                    // the pair's v, floors, v lerps and accumulations on
-                    // f32x2 values (sm_100 packed FP32): the same operations
-                    // on each half, so the same bits
-                    const float2 dlv2 = make_float2(dlv, dlv), lv02 = make_float2(lv0, lv0);
-                    const float2 rw22 = make_float2(rw2, rw2);
-#pragma unroll
-                    for (int z = 0; z < TB_Z; z += 2) {
-                        const float2 l = __ffma2_rn(make_float2((float)z, (float)(z + 1)), dlv2, lv02);
-                        const FloorFrac2 f = floor_frac2(l);
-                        unsigned idx = (unsigned)f.bits0 * (unsigned)BOX_W + col;
-                        idx = min(idx, MAX_IDX2);  // memory safety only: the margin keeps idx in range
-                        const float p0 = smem_ulerp(tile + idx, tx), p1 = smem_ulerp(tile + idx + BOX_W, tx);
-                        const float p2 = smem_ulerp(tile + idx + 2 * BOX_W, tx);
-                        const bool up = f.bits1 != f.bits0;
-                        const float2 lo = make_float2(p0, up ? p1 : p0), hi = make_float2(p1, up ? p2 : p1);
-                        const float2 nf = __ffma2_rn(f.f, make_float2(-1.0f, -1.0f), make_float2(0.0f, 0.0f));
-                        float2 a = make_float2(acc[z], acc[z + 1]);
-                        a = __ffma2_rn(lerp_ref2(lo, hi, f.f, nf), rw22, a);
-                        acc[z] = a.x;
-                        acc[z + 1] = a.y;
-                    }
-#else
 #pragma unroll
                     for (int z = 0; z < TB_Z; z += 2) {
                         const float la = fmaf((float)z, dlv, lv0), lb = fmaf((float)(z + 1), dlv, lv0);
@@ -344,7 +297,6 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
                         const bool up = fb.bits != fa.bits;
                         acc[z + 1] = fmaf(lerp_ref(up ? p1 : p0, up ? p2 : p1, fb.f), rw2, acc[z + 1]);
                     }
-#endif
                 } else {
 #pragma unroll
                     for (int z = 0; z < TB_Z; ++z) {
@@ -462,7 +414,7 @@ cudaError_t launch_typed(const void *sinogram, void *volume, const Dims3D &d, co
     const dim3 block(TB_X, TB_Y, 1);
     const dim3 grid((d.vol_x + TB_X - 1) / TB_X, (d.vol_y + TB_Y - 1) / TB_Y, zblocks * d.batch);
     static_assert((BOX_ELEMS * sizeof(float)) % 128 == 0 && (BOX_ELEMS * 2) % 128 == 0, "tile alignment");
-    const size_t smem = 2 * BpViews<Tin>::K * BOX_ELEMS * sizeof(Tin) + 128;
+    const size_t smem = 2 * BP_K * BOX_ELEMS * sizeof(Tin) + 128;
     // set on every launch: the attribute belongs to the current device's copy
     // of the kernel, and the call is a cheap host-side update
     cudaError_t e = cudaFuncSetAttribute(cone_bp_tma_kernel<Tin, Tout>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -29,9 +29,13 @@
 //
 // No TMA and no multicast: every operand byte is written by the CTA's own
 // threads.  Waits are bounded: a wait that gives up records
-// DEVICE_ERROR_MBARRIER_TIMEOUT in g_fdk_error (read by pyronn_fdk_error), and
-// the CTA stops building operands, waits (again bounded) for the MMAs of its
-// last committed chunk, frees its TMEM and exits without storing its tile.
+// DEVICE_ERROR_MBARRIER_TIMEOUT in g_fdk_error (read by pyronn_fdk_error); the
+// thread then tries its later waits once each, thread 0 issues no more MMAs,
+// every thread still walks every chunk (same barriers, no early exit; the
+// operands it keeps writing may race with MMAs in flight, and the tile is
+// not stored), a failed final wait is waited for again (bounded) before the
+// TMEM is freed, and a warp with any failed wait stores nothing.  Skipping
+// the operand writes after a failure instead cost 4 % of the filter's time.
 #include <type_traits>
 
 #include "common.cuh"
@@ -181,11 +185,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ uint64_t mma_done[2];  // stage s free again: its MMAs are done
     __shared__ uint32_t tmem_slot;
-    // a thread's wait for chunk c gave up: flag c & 1 (two flags, so a flag
-    // is read after the chunk's barrier before any thread can write it for a
-    // later chunk -- the break below is the same for every thread); flag 2:
-    // the final wait
-    __shared__ int s_failed[3];
     __shared__ float vv2[TC_N];  // per row of the tile: (v - cv)^2 dv^2 of its detector row
     unsigned char *base = smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u);
     // the tile's taps tau h[m], m = j0 + jj - k over jj < 128, k < Wk, in
@@ -221,7 +220,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         mbar_init(&mma_done[0], 1);
         mbar_init(&mma_done[1], 1);
         fence_mbar_init();
-        s_failed[0] = s_failed[1] = s_failed[2] = 0;
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
@@ -250,7 +248,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         bnext[i] = (brow[i] && 4 * bq[i] < W) ? Quad<Tin>::load(bptr[i]) : Quad<Tin>::zero();
     }
     const int nK = Wk / TC_K;
-    int nc = 0;  // chunks whose MMAs were issued
+    bool failed = false;  // one of this thread's waits gave up
     for (int c = 0; c < nK; ++c) {
         const int s = c & 1;
         typename Quad<Tin>::raw bcur[BG];
@@ -261,14 +259,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             if (c + 1 < nK) bnext[i] = (brow[i] && kn < W) ? Quad<Tin>::load(bptr[i] + (c + 1) * TC_K) : Quad<Tin>::zero();
         }
         unsigned char *st = base + s * STAGE_BYTES;
-        // a thread whose wait gave up leaves the stage alone: MMAs may still read it
-        const bool ok = c < 2 || mbar_wait_bounded(&mma_done[s], ((c - 2) >> 1) & 1, &g_fdk_error);
-        if (!ok) s_failed[c & 1] = 1;
+        // after a wait gave up the thread tries its later waits once each
+        if (c >= 2 && !mbar_wait_bounded(&mma_done[s], ((c - 2) >> 1) & 1, &g_fdk_error, failed ? 1u : (1u << 22)))
+            failed = true;
         const int k0 = c * TC_K;
         // 16-byte chunks: g = row * 8 + q, inputs k0 + 4q .. k0 + 4q + 3; a
         // warp covers 4 rows x 8 chunks (512 contiguous bytes when stored)
 #pragma unroll
-        for (int i = 0; i < (TC_M * TC_K / 4) / TC_THREADS && ok; ++i) {
+        for (int i = 0; i < (TC_M * TC_K / 4) / TC_THREADS; ++i) {
             // A = T chunk, row jj (output j0 + jj)
             const int g = tid + i * TC_THREADS, jj = g >> 3, q = g & 7;
             const int x0 = TC_M - 1 - jj + k0 + 4 * q, al = x0 & 3;
@@ -279,7 +277,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             *reinterpret_cast<float4 *>(st + A_BYTES + off) = lo;
         }
 #pragma unroll
-        for (int i = 0; i < BG && ok; ++i) {
+        for (int i = 0; i < BG; ++i) {
             // B = G chunk, row rr (detector row r0 + rr); W is a multiple of
             // 4, so a chunk's four inputs are all inside the row or all zero
             const int rr = brr[i], q = bq[i];
@@ -304,8 +302,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // 4.7 -> 5.4 ms on the 512^3 workload's rows)
         fence_proxy_async_smem();
         __syncthreads();
-        if (s_failed[c & 1]) break;
-        if (tid == 0) {
+        if (tid == 0 && !failed) {
             tc_fence_after();
             const uint32_t a = smem_addr(st), b = smem_addr(st + 2 * A_BYTES);
             const uint32_t acc = tmem_d + (uint32_t)((c % NACC) * TC_N);
@@ -320,23 +317,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             }
             umma_commit(&mma_done[s]);
         }
-        nc = c + 1;
     }
     // the last commit arrives once every MMA of the tile is done
-    const bool broke = nc < nK;  // the same for every thread
-    if (!broke && !mbar_wait_bounded(&mma_done[(nK - 1) & 1], ((nK - 1) >> 1) & 1, &g_fdk_error)) s_failed[2] = 1;
-    __syncthreads();
-    if (broke || s_failed[2]) {
-        // MMAs may still be in flight: wait (bounded) for the last commit
-        // before the TMEM is freed; the tile is not stored
-        if (tid == 0 && nc > 0) mbar_wait_bounded(&mma_done[(nc - 1) & 1], ((nc - 1) >> 1) & 1, nullptr);
-        tc_fence_before();
-        __syncthreads();
-        if (warp == 0)
-            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(TMEM_COLS)
-                         : "memory");
-        return;
-    }
+    const bool done = !failed && mbar_wait_bounded(&mma_done[(nK - 1) & 1], ((nK - 1) >> 1) & 1, &g_fdk_error);
+    // MMAs may still be in flight: thread 0 waits for them again (bounded)
+    // before the barrier that precedes the TMEM's release
+    if (!done && tid == 0) mbar_wait_bounded(&mma_done[(nK - 1) & 1], ((nK - 1) >> 1) & 1, nullptr);
     tc_fence_after();
 
     // epilogue: warp w reads TMEM lane quadrant w % 4 (outputs
@@ -347,7 +333,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const int j = j0 + 32 * quad + lane;
     const float uu = ((float)j - cu) * du;
     const int nacc = nK < NACC ? nK : NACC;
-    {
+    if (__all_sync(0xffffffffu, done)) {  // warp-uniform: tcgen05.ld is .sync.aligned
         const int q = warp >> 2;
         float sum[32];
         for (int a = 0; a < nacc; ++a) {

@@ -346,7 +346,7 @@ struct RowTaps<float> {
 // differs from the exact one: its denominator below 1e-6 gives NaN, which the
 // texture unit samples as coordinate 0 (measured on B200: half of the view's
 // first texel, i.e. index -0.5); just above it, a far-off point.
-__device__ __noinline__ float fan_index_reference_steps(float cx, float cy, float rx, float ry, float sid, float sdd,
+__device__ __forceinline__ float fan_index_reference_steps(float cx, float cy, float rx, float ry, float sid, float sdd,
                                                         float dorg, float ds)
 {
     const float srcx = __fmul_rn(rx, -sid), srcy = __fmul_rn(ry, -sid);
@@ -369,7 +369,13 @@ __device__ __noinline__ float fan_index_reference_steps(float cx, float cy, floa
 // constants the block first puts in shared memory (one view per thread):
 // parallel beam (-r.y, r.x) / detector spacing, fan beam (r.x, r.y, SID |r|^2,
 // SDD |r|^2 / detector spacing), so a view costs each pixel one broadcast load.
-template <typename T, typename Tout, bool FAN>
+// Fan beam: a geometry in which some view's source depth line comes within
+// 2e-2 mm of the slice (the source inside or at the field) needs the
+// reference's FP32 steps near that line (fan_index_reference_steps), which
+// would cost the common case registers and occupancy; two instantiations are
+// launched instead, NEAR_DEPTH = false and true, and each block checks the
+// geometry first and leaves the work to the instantiation that matches it.
+template <typename T, typename Tout, bool FAN, bool NEAR_DEPTH>
 __global__ void __launch_bounds__(BP2_BLOCK_X *BP2_BLOCK_Y)
     backprojection2d_kernel(const T *__restrict__ sino, Tout *__restrict__ vol, Geom2D geo, int X, int Y, int W,
                             int n_proj, int geom_batch)
@@ -383,17 +389,29 @@ __global__ void __launch_bounds__(BP2_BLOCK_X *BP2_BLOCK_Y)
     const int g = geom_batch == 1 ? 0 : b;
     const float sx = geo.volume_spacing[2 * g + 1], sy = geo.volume_spacing[2 * g + 0];
     const float ox = geo.volume_origin[2 * g + 1], oy = geo.volume_origin[2 * g + 0];
-    const float ds = geo.detector_spacing[g], dorg = geo.detector_origin[g];
-    const float ids = 1.0f / ds;
-    const float sdo = dorg * ids;  // detector origin in pixels
-    const float cx = (float)i * sx + ox, cy = (float)j * sy + oy;
     const float2 *rays = reinterpret_cast<const float2 *>(geo.rays) + (size_t)g * n_proj;
-    const T *sino_b = sino + (size_t)b * n_proj * W;
     float sid = 0.0f, sdd = 0.0f;
     if (FAN) {
         sid = geo.sid[g];
         sdd = geo.sdd[g];
+        // a view's depth <c - src, r> is affine in the pixel centre c, so its
+        // extremes over the slice are at the corners of the pixel-centre box
+        const float x0 = ox, x1 = ox + (float)(X - 1) * sx, y0 = oy, y1 = oy + (float)(Y - 1) * sy;
+        bool near = false;
+        for (int n = tid; n < n_proj; n += BP2_BLOCK_X * BP2_BLOCK_Y) {
+            const float2 r = __ldg(&rays[n]);
+            const float base = sid * (r.x * r.x + r.y * r.y);
+            const float d0 = fmaf(x0, r.x, fmaf(y0, r.y, base)), d1 = fmaf(x1, r.x, fmaf(y0, r.y, base));
+            const float d2 = fmaf(x0, r.x, fmaf(y1, r.y, base)), d3 = fmaf(x1, r.x, fmaf(y1, r.y, base));
+            near |= fminf(fminf(d0, d1), fminf(d2, d3)) < 2.0e-2f && fmaxf(fmaxf(d0, d1), fmaxf(d2, d3)) > -2.0e-2f;
+        }
+        if (__syncthreads_or(near) != NEAR_DEPTH) return;  // the other instantiation's block
     }
+    const float ds = geo.detector_spacing[g], dorg = geo.detector_origin[g];
+    const float ids = 1.0f / ds;
+    const float sdo = dorg * ids;  // detector origin in pixels
+    const float cx = (float)i * sx + ox, cy = (float)j * sy + oy;
+    const T *sino_b = sino + (size_t)b * n_proj * W;
     float acc = 0.0f;
     for (int n0 = 0; n0 < n_proj; n0 += BP2_CHUNK) {
         const int cnt = min(BP2_CHUNK, n_proj - n0);
@@ -411,7 +429,7 @@ __global__ void __launch_bounds__(BP2_BLOCK_X *BP2_BLOCK_Y)
         __syncthreads();
         if (!live) continue;
         const T *row = sino_b + (size_t)n0 * W;
-#pragma unroll 4
+#pragma unroll(NEAR_DEPTH ? 1 : 4)
         for (int k = 0; k < cnt; ++k, row += W) {
             const float4 q = tab[k];
             float sidx, w = 1.0f;
@@ -425,9 +443,9 @@ __global__ void __launch_bounds__(BP2_BLOCK_X *BP2_BLOCK_Y)
                 const float cr = fmaf(cx, q.x, cy * q.y);
                 const float den = cr + q.z;  // <c - src, r>: the pixel's depth from the source
                 sidx = fmaf(q.w * cd, fast_rcp(den), -sdo);
-                // within 1e-2 mm of the source's depth, the reference's FP32
-                // steps decide (rare: the source inside or at the field)
-                if (fabsf(den) < 1.0e-2f) sidx = fan_index_reference_steps(cx, cy, q.x, q.y, sid, sdd, dorg, ds);
+                // within 1e-2 mm of the source's depth, the reference's FP32 steps decide
+                if (NEAR_DEPTH && fabsf(den) < 1.0e-2f)
+                    sidx = fan_index_reference_steps(cx, cy, q.x, q.y, sid, sdd, dorg, ds);
                 const float ex = fmaf(q.x, sid, cx), ey = fmaf(q.y, sid, cy);
                 w = fast_rcp(fmaf(ex, ex, ey * ey));
             }
@@ -520,12 +538,16 @@ cudaError_t bp_typed(const void *sinogram, void *volume, bool fan, const Dims2D 
     const dim3 block(BP2_BLOCK_X, BP2_BLOCK_Y);
     const dim3 grid((d.vol_x + BP2_BLOCK_X - 1) / BP2_BLOCK_X, (d.vol_y + BP2_BLOCK_Y - 1) / BP2_BLOCK_Y,
                     d.batch);
-    if (fan)
-        backprojection2d_kernel<Tin, Tout, true><<<grid, block, 0, stream>>>(
+    if (fan) {
+        // every block runs in exactly one of the two (see the kernel)
+        backprojection2d_kernel<Tin, Tout, true, false><<<grid, block, 0, stream>>>(
             (const Tin *)sinogram, (Tout *)volume, g, d.vol_x, d.vol_y, d.det_w, d.n_proj, d.geom_batch);
-    else
-        backprojection2d_kernel<Tin, Tout, false><<<grid, block, 0, stream>>>(
+        backprojection2d_kernel<Tin, Tout, true, true><<<grid, block, 0, stream>>>(
             (const Tin *)sinogram, (Tout *)volume, g, d.vol_x, d.vol_y, d.det_w, d.n_proj, d.geom_batch);
+    } else {
+        backprojection2d_kernel<Tin, Tout, false, false><<<grid, block, 0, stream>>>(
+            (const Tin *)sinogram, (Tout *)volume, g, d.vol_x, d.vol_y, d.det_w, d.n_proj, d.geom_batch);
+    }
     return cudaGetLastError();
 }
 
