@@ -328,9 +328,11 @@ def reference_gpu(cfg, geo, vol32, dev, f_ms, b_ms, ours_fp32_gups, ours_gups, a
     per-call allocations and FP32 storage, the reference's
     Cone_Projection_Kernel_Launcher (cone_projector_3D_CudaKernel.cu.cc:225-257)
     and Cone_Backprojection3D_Kernel_Launcher
-    (cone_backprojector_3D_CudaKernel.cu.cc:121-146) -- on this workload,
-    timed with CUDA events on the default stream; outside our timed regions.
-    Also the relative L2 distance of our FP32 results from theirs."""
+    (cone_backprojector_3D_CudaKernel.cu.cc:121-146), or their texture
+    launchers (..._hardware_interp.cu.cc) for a --hardware-interp run -- on
+    this workload, timed with CUDA events on the default stream; outside our
+    timed regions.  Also the relative L2 distance of our FP32 results from
+    theirs."""
     import ctypes
 
     import torch
@@ -338,8 +340,7 @@ def reference_gpu(cfg, geo, vol32, dev, f_ms, b_ms, ours_fp32_gups, ours_gups, a
     import oracle
     if not os.path.exists(oracle.REF_LIB):
         return {"unavailable": "oracle/_ref/libpyronn_ref.so not built (needs the reference sources)"}
-    if args.hardware_interp:
-        return {"unavailable": "timed for the software-interpolation workload only"}
+    hw = 1 if args.hardware_interp else 0
     L = ctypes.CDLL(oracle.REF_LIB)
     Z, Y, X = cfg["volume"]
     H, W = cfg["detector"]
@@ -358,9 +359,9 @@ def reference_gpu(cfg, geo, vol32, dev, f_ms, b_ms, ours_fp32_gups, ours_gups, a
     vol = vol32[None].contiguous()
     sino = torch.zeros(n * H * W + W + 8, dtype=torch.float32, device=dev)  # slack for its x == W taps
     back = torch.zeros(Z * Y * X, dtype=torch.float32, device=dev)
-    fargs = (ctypes.c_void_p(vol.data_ptr()), ctypes.c_void_p(sino.data_ptr()), 0, 1, Z, Y, X, n, H, W, g[0], g[1],
+    fargs = (ctypes.c_void_p(vol.data_ptr()), ctypes.c_void_p(sino.data_ptr()), hw, 1, Z, Y, X, n, H, W, g[0], g[1],
              g[2], g[3])
-    bargs = (ctypes.c_void_p(sino.data_ptr()), ctypes.c_void_p(back.data_ptr()), 0, 1, n, H, W, Z, Y, X, g[0], g[1],
+    bargs = (ctypes.c_void_p(sino.data_ptr()), ctypes.c_void_p(back.data_ptr()), hw, 1, n, H, W, Z, Y, X, g[0], g[1],
              g[2], g[4])
 
     def timed(fn, reps=2):
@@ -384,13 +385,14 @@ def reference_gpu(cfg, geo, vol32, dev, f_ms, b_ms, ours_fp32_gups, ours_gups, a
         return {"unavailable": str(exc)}
     # our FP32 results on the same inputs, for the parity figure at this size
     from pyronn_layers import ops
-    ours_s = ops.cone_projection3d(vol, geo.detector_shape, *geo.args())
+    ours_s = ops.cone_projection3d(vol, geo.detector_shape, *geo.args(), hardware_interp=bool(hw))
     e_f = rel_l2(ours_s.reshape(-1).cpu().numpy(), sino[: n * H * W].cpu().numpy())
-    ours_v = ops.cone_backprojection3d(sino[: n * H * W].reshape(1, n, H, W), geo.volume_shape, *geo.args())
+    ours_v = ops.cone_backprojection3d(sino[: n * H * W].reshape(1, n, H, W), geo.volume_shape, *geo.args(),
+                                       hardware_interp=bool(hw))
     e_b = rel_l2(ours_v.reshape(-1).cpu().numpy(), back.cpu().numpy())
     gups = 2 * updates(cfg) / ((fms + bms) / 1e3) / 1e9
     return {"value": gups, "unit": "GUPS", "forward_ms": fms, "backprojection_ms": bms,
-            "storage": "fp32 (the reference's only storage type)",
+            "storage": "fp32 (the reference's only storage type)", "hardware_interp": bool(hw),
             "ours_fp32_over_reference": ours_fp32_gups / gups, "ours_over_reference": ours_gups / gups,
             "forward_over_reference": fms / f_ms, "backprojection_over_reference": bms / b_ms,
             "ours_fp32_forward_rel_l2_vs_reference": e_f, "ours_fp32_backprojection_rel_l2_vs_reference": e_b,
@@ -880,49 +882,181 @@ def run_serving_sweep(args):
     print(json.dumps(line))
 
 
-FAN2D = dict(batch=64, volume=(512, 512), pixel_mm=0.5, views=360, detector=1024, det_mm=0.5, sid_mm=750.0,
-             sdd_mm=1200.0)
+FAN2D = dict(kind="fan", batch=64, volume=(512, 512), pixel_mm=0.5, views=360, detector=1024, det_mm=0.5,
+             sid_mm=750.0, sdd_mm=1200.0, min_steps=1, accuracy_slices=1)
+# one 256^2 slice per step; the tiny step is launch-bound, so a batch of
+# slices per call is timed beside it (`batched`), and at least 200 steps are
+# timed for a stable CUDA-event time
+PAR2D = dict(kind="parallel", batch=1, volume=(256, 256), pixel_mm=1.0, views=180, detector=367, det_mm=1.0,
+             min_steps=200, batched=256, accuracy_slices=1)
+WORKLOADS_2D = {"fan2d": FAN2D, "par2d": PAR2D}
 
 
-def run_fan2d(args):
-    """2D fan-beam batch (config 2): 64 independent 512^2 slices at 0.5 mm,
-    360 views over 2 pi, flat 1024-px detector at 0.5 mm, SID 750 / SDD 1200;
-    one step = FanProjection2D of the batch + FanBackprojection2D of its
-    sinograms.  GUPS = 2 * 64 * 512^2 * 360 / t."""
+def geometry_2d(c):
+    from pyronn_layers import geometry
+    if c["kind"] == "fan":
+        return geometry.FanBeam2D(c["volume"], (c["pixel_mm"],) * 2, c["detector"], c["det_mm"], c["views"],
+                                  c["sid_mm"], c["sdd_mm"])
+    return geometry.ParallelBeam2D(c["volume"], (c["pixel_mm"],) * 2, c["detector"], c["det_mm"], c["views"])
+
+
+def reference_gpu_2d(c, g, vols, dev, ours, ours_fp32_gups, ours_gups):
+    """The reference's own 2D kernels (cc/kernels/{par,fan}_{projector,
+    backprojector}_2D_CudaKernel.cu.cc built unmodified into oracle/_ref by the
+    oracle's recipe) through the op-layer restatement oracle/ref/ref_driver.cu:
+    one launcher call per batch element, as the reference's ops loop
+    (cc/ops/par_projector_2D_OPKernel.cc, fan_projector_2D_OPKernel.cc), FP32,
+    default stream, 1 warm-up + 2 timed calls per op; outside our timed
+    regions.  `ours` = (forward ms, backprojection ms, FP32 sinogram, FP32
+    volume) of our kernels on the same FP32 inputs, for the ratios and the
+    relative L2 distance of our results from theirs."""
+    import ctypes
+
     import torch
 
-    from pyronn_layers import geometry, ops, phantoms
+    import oracle
+    if not os.path.exists(oracle.REF_LIB):
+        return {"unavailable": "oracle/_ref/libpyronn_ref.so not built (needs the reference sources)"}
+    L = ctypes.CDLL(oracle.REF_LIB)
+    B, (Y, X), n, W = c["batch"], c["volume"], c["views"], c["detector"]
+    keep = []
+
+    def dptr(a):
+        t = torch.from_numpy(np.ascontiguousarray(np.asarray(a, dtype=np.float32)).reshape(-1)).to(dev)
+        keep.append(t)
+        return ctypes.c_void_p(t.data_ptr())
+
+    def rows(a):
+        return dptr(np.repeat(np.asarray(a, np.float32).reshape(1, -1), B, axis=0))
+
+    geo = [rows(g.volume_origin), rows(g.detector_origin), rows(g.volume_spacing), rows(g.detector_spacing)]
+    if c["kind"] == "fan":
+        geo += [rows(g.sid), rows(g.sdd)]
+    geo.append(rows(g.ray_vectors))
+    vol = torch.from_numpy(np.ascontiguousarray(vols, dtype=np.float32)).to(dev)
+    sino = torch.zeros(B * n * W, dtype=torch.float32, device=dev)
+    back = torch.zeros(B * Y * X, dtype=torch.float32, device=dev)
+    fwd = L.ref_fan_projection2d if c["kind"] == "fan" else L.ref_parallel_projection2d
+    bwd = L.ref_fan_backprojection2d if c["kind"] == "fan" else L.ref_parallel_backprojection2d
+    fargs = (ctypes.c_void_p(vol.data_ptr()), ctypes.c_void_p(sino.data_ptr()), B, Y, X, n, W, *geo)
+    bargs = (ctypes.c_void_p(sino.data_ptr()), ctypes.c_void_p(back.data_ptr()), B, n, W, Y, X, *geo)
+
+    def timed(fn, reps=2):
+        if fn() != 0:
+            raise RuntimeError("reference launcher failed")
+        times = []
+        for _ in range(reps):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            fn()
+            e.record()
+            torch.cuda.synchronize()
+            times.append(s.elapsed_time(e))
+        return statistics.mean(times)
+
+    try:
+        fms = timed(lambda: fwd(*fargs))
+        ref_sino = sino.clone()
+        # their backprojection of OUR FP32 sinogram, so both backprojections
+        # see the same input
+        sino.copy_(ours[2].reshape(-1))
+        bms = timed(lambda: bwd(*bargs))
+    except RuntimeError as exc:
+        return {"unavailable": str(exc)}
+    gups = 2 * B * Y * X * n / ((fms + bms) / 1e3) / 1e9
+    return {"value": gups, "unit": "GUPS", "forward_ms": fms, "backprojection_ms": bms,
+            "storage": "fp32 (the reference's only storage type)", "hardware_interp": bool(hw),
+            "ours_fp32_over_reference": ours_fp32_gups / gups, "ours_over_reference": ours_gups / gups,
+            "ours_fp32_forward_rel_l2_vs_reference": rel_l2(ours[2].reshape(-1).cpu().numpy(),
+                                                            ref_sino.cpu().numpy()),
+            "ours_fp32_backprojection_rel_l2_vs_reference": rel_l2(ours[3].reshape(-1).cpu().numpy(),
+                                                                   back.cpu().numpy()),
+            "what": "the reference's own 2D kernels (built unmodified for sm_100a) through a restatement of its TF "
+                    "op layer (oracle/ref/ref_driver.cu): one launcher call per batch element, FP32, default "
+                    "stream, 1 warm-up + 2 timed calls per op"}
+
+
+def run_2d(args):
+    """2D workloads.  fan2d (config 2): 64 independent 512^2 slices at
+    0.5 mm, 360 views over 2 pi, flat 1024-px detector at 0.5 mm, SID 750 /
+    SDD 1200.  par2d (config 1): one 256^2 slice at 1.0 mm, 180 views over
+    pi, 367-px detector at 1.0 mm.  One step = the projection of the batch +
+    the backprojection of its sinograms; GUPS = 2 * batch * slice pixels *
+    views / t.  Beside it: the plain FP32 path, the relative L2 error of the
+    first slice against the FP64 oracle, and the reference's own kernels."""
+    import torch
+
+    from pyronn_layers import ops, phantoms
     if int(os.environ.get("RANK", "0")) != 0:
         return
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
-    c = FAN2D
-    g = geometry.FanBeam2D(c["volume"], (c["pixel_mm"],) * 2, c["detector"], c["det_mm"], c["views"], c["sid_mm"],
-                           c["sdd_mm"])
-    vols = np.stack([phantoms.ellipse_phantom_2d(c["volume"], (c["pixel_mm"],) * 2, seed=100 + b)[0]
+    c = WORKLOADS_2D[args.workload]
+    fan = c["kind"] == "fan"
+    g = geometry_2d(c)
+    seed0 = 100 if fan else 1
+    vols = np.stack([phantoms.ellipse_phantom_2d(c["volume"], (c["pixel_mm"],) * 2, seed=seed0 + b)[0]
                      for b in range(c["batch"])])
     storage = {"bf16": torch.bfloat16, "fp16": torch.float16, "fp32": torch.float32}[args.storage]
-    units = c["batch"] * c["volume"][0] * c["volume"][1] * c["views"]
+    steps = max(args.steps, c["min_steps"])
+    lib = ops._capi
+    fwd_name = "pyronn_fan_projection2d" if fan else "pyronn_parallel_projection2d"
+    bwd_name = "pyronn_fan_backprojection2d" if fan else "pyronn_parallel_backprojection2d"
+    geo_extra = (g.sid, g.sdd) if fan else ()
 
-    def run(store):
-        x = torch.from_numpy(vols).to(dev, store)
-        geo = ops.Geometry2D(c["batch"], dev, *g.args()[:4], g.ray_vectors, c["views"], g.sid, g.sdd)
-        sino = torch.empty((c["batch"], c["views"], c["detector"]), dtype=store, device=dev)
-        back = torch.empty((c["batch"],) + c["volume"], dtype=torch.float32, device=dev)
+    def run(store, batch_vols, graph=False):
+        B = batch_vols.shape[0]
+        units = B * c["volume"][0] * c["volume"][1] * c["views"]
+        x = torch.from_numpy(batch_vols).to(dev, store)
+        geo = ops.Geometry2D(B, dev, *g.args()[:4], g.ray_vectors, c["views"], *geo_extra)
+        sino = torch.empty((B, c["views"], c["detector"]), dtype=store, device=dev)
+        back = torch.empty((B,) + c["volume"], dtype=torch.float32, device=dev)
         code = ops.storage_code(store)
-        lib = ops._capi
-        ws = torch.empty(lib.workspace_size("pyronn_projection2d", c["batch"], *c["volume"], code),
-                         dtype=torch.uint8, device=dev)
+        ws = torch.empty(lib.workspace_size("pyronn_projection2d", B, *c["volume"], code), dtype=torch.uint8,
+                         device=dev)
         ev = []
+
+        def launch_fwd(s):
+            lib.call(fwd_name, x.data_ptr(), sino.data_ptr(), code, code, B, *c["volume"], c["views"],
+                     c["detector"], *geo.pointers(), geo.g, ws.data_ptr(), ws.numel(), s)
+
+        def launch_bwd(s):
+            lib.call(bwd_name, sino.data_ptr(), back.data_ptr(), code, 0, B, c["views"], c["detector"],
+                     *c["volume"], *geo.pointers(), geo.g, s)
+
+        if graph:
+            # one step captured as a CUDA graph and replayed: the step without
+            # the host's per-call cost
+            side = torch.cuda.Stream(dev)
+            with torch.cuda.stream(side):
+                for _ in range(args.warmup):
+                    launch_fwd(side.cuda_stream)
+                    launch_bwd(side.cuda_stream)
+            torch.cuda.synchronize(dev)
+            cg = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(cg, stream=side):
+                launch_fwd(side.cuda_stream)
+                launch_bwd(side.cuda_stream)
+            for _ in range(args.warmup):
+                cg.replay()
+            torch.cuda.synchronize(dev)
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record()
+            for _ in range(steps):
+                cg.replay()
+            t1.record()
+            torch.cuda.synchronize(dev)
+            ms = t0.elapsed_time(t1)
+            del cg
+            ops.check_device_errors(dev)
+            return {"gups": 2 * units * steps / (ms / 1e3) / 1e9, "ms": ms}
 
         def step():
             e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
             s = torch.cuda.current_stream(dev).cuda_stream
             e[0].record()
-            lib.call("pyronn_fan_projection2d", x.data_ptr(), sino.data_ptr(), code, code, c["batch"],
-                     *c["volume"], c["views"], c["detector"], *geo.pointers(), geo.g, ws.data_ptr(), ws.numel(), s)
+            launch_fwd(s)
             e[1].record()
-            lib.call("pyronn_fan_backprojection2d", sino.data_ptr(), back.data_ptr(), code, 0, c["batch"],
-                     c["views"], c["detector"], *c["volume"], *geo.pointers(), geo.g, s)
+            launch_bwd(s)
             e[2].record()
             ev.append(e)
 
@@ -932,27 +1066,72 @@ def run_fan2d(args):
         ev.clear()
         t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0.record()
-        for _ in range(args.steps):
+        for _ in range(steps):
             step()
         t1.record()
         torch.cuda.synchronize()
         ms = t0.elapsed_time(t1)
         f = statistics.mean(a.elapsed_time(b) for a, b, _ in ev)
         bk = statistics.mean(b.elapsed_time(c2) for _, b, c2 in ev)
-        return 2 * units * args.steps / (ms / 1e3) / 1e9, ms, f, bk, sino, back
+        ops.check_device_errors(dev)
+        return {"gups": 2 * units * steps / (ms / 1e3) / 1e9, "ms": ms, "forward_ms": f, "backprojection_ms": bk,
+                "sino": sino, "back": back}
 
     with ClockSampler(physical_gpu_index(dev.index or 0)) as clk:
-        gups, ms, f_ms, b_ms, sino, back = run(storage)
-    gups32 = run(torch.float32)[0] if storage != torch.float32 else None
+        r = run(storage, vols)
+    r32 = run(torch.float32, vols) if storage != torch.float32 else r
+    batched = None
+    if c.get("batched"):
+        rb = run(storage, np.repeat(vols[:1], c["batched"], axis=0))
+        batched = {"value": rb["gups"], "unit": "GUPS", "slices_per_call": c["batched"],
+                   "forward_ms": rb["forward_ms"], "backprojection_ms": rb["backprojection_ms"],
+                   "note": "the same slice repeated, %d per call: the kernels' throughput without the per-call "
+                           "launch cost that bounds the one-slice step" % c["batched"]}
+        del rb
+        rg = run(storage, vols, graph=True)
+        batched["one_slice_graph_replay"] = {"value": rg["gups"], "unit": "GUPS", "ms_per_step": rg["ms"] / steps,
+                                             "note": "the one-slice step captured once as a CUDA graph and replayed "
+                                                     "%d times" % steps}
+
+    def accuracy(res):
+        import oracle
+        k = c["accuracy_slices"]
+        v = vols[:k]
+        geo_args = g.args()
+        if fan:
+            ref_s = oracle.fan_projection2d(v, g.detector_shape, *geo_args)
+        else:
+            ref_s = oracle.parallel_projection2d(v, g.detector_shape, *geo_args)
+        ours_s = res["sino"][:k].float().cpu().numpy()
+        # the oracle backprojects our sinogram: the backprojection's own error
+        if fan:
+            ref_b = oracle.fan_backprojection2d(ours_s, c["volume"], *geo_args)
+        else:
+            ref_b = oracle.parallel_backprojection2d(ours_s, c["volume"], *geo_args)
+        return {"forward_rel_l2_vs_fp64": rel_l2(ours_s.reshape(-1), ref_s.reshape(-1)),
+                "backprojection_rel_l2_vs_fp64": rel_l2(res["back"][:k].cpu().numpy().reshape(-1),
+                                                        ref_b.reshape(-1)),
+                "slices": k}
+
+    acc = {args.storage: accuracy(r)}
+    if r32 is not r:
+        acc["fp32"] = accuracy(r32)
+    acc["note"] = ("forward: our sinogram of the first slice (stored as named) against the FP64 oracle on the FP32 "
+                   "phantom; backprojection: the FP64 oracle's backprojection of the same sinogram")
+    ref = reference_gpu_2d(c, g, vols, dev, (r32["forward_ms"], r32["backprojection_ms"], r32["sino"], r32["back"]),
+                           r32["gups"], r["gups"])
     line = {
-        "metric": METRIC, "value": gups, "unit": "GUPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "metric": METRIC, "value": r["gups"], "unit": "GUPS", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": r["ms"] / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "storage": args.storage, "data": "synthetic",
-        "config": {"workload": "fan2d", "batch": c["batch"], "slice": list(c["volume"]), "pixel_mm": c["pixel_mm"],
-                   "views": c["views"], "detector_px": c["detector"], "det_mm": c["det_mm"], "sid_mm": c["sid_mm"],
-                   "sdd_mm": c["sdd_mm"], "phantom": "10 seeded ellipses per slice"},
-        "plain_fp32_value": gups32,
-        "kernels": {"forward_ms": f_ms, "backprojection_ms": b_ms},
+        "config": {"workload": args.workload, "geometry": c["kind"], "batch": c["batch"],
+                   "slice": list(c["volume"]), "pixel_mm": c["pixel_mm"], "views": c["views"],
+                   "detector_px": c["detector"], "det_mm": c["det_mm"],
+                   **({"sid_mm": c["sid_mm"], "sdd_mm": c["sdd_mm"]} if fan else {}),
+                   "phantom": "10 seeded ellipses per slice"},
+        "plain_fp32_value": r32["gups"],
+        "kernels": {"forward_ms": r["forward_ms"], "backprojection_ms": r["backprojection_ms"]},
+        "accuracy": acc, "batched": batched, "reference_gpu": ref,
         "clocks": clk.summary(),
     }
     print(json.dumps(line))
@@ -1176,7 +1355,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving", "serving-sweep", "fan2d", "fdk", "diffcone"],
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["serving", "serving-sweep", "fan2d", "par2d", "fdk", "diffcone"],
                     default="cone512")
 
     ap.add_argument("--requests", type=int, default=2000, help="serving: number of requests")
@@ -1196,11 +1375,13 @@ def main(argv=None):
                     help="dram bytes per launch of the dominant kernel from an ncu capture")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)  # at least 3 untimed warm-up steps
-    if args.workload == "fan2d":
+    if args.workload in WORKLOADS_2D:
         if args.impl == "reference":
-            print(json.dumps({"impl": "reference", "unavailable": "the fan2d workload is measured on the GPU arm only"}))
+            print(json.dumps({"impl": "reference", "unavailable": "the 2D workloads are measured on the GPU arm "
+                                                                   "only (their reference_gpu block times the "
+                                                                   "reference's kernels)"}))
             return
-        run_fan2d(args)
+        run_2d(args)
         return
     if args.workload == "diffcone":
         if args.impl == "reference":
