@@ -88,8 +88,9 @@ __device__ __forceinline__ float sub_f32_bf16(unsigned w, float c)
 
 // The first-axis lerp of a storage type's taps, on values already widened to
 // FP32: the reference's form for FP32 storage, a + t (b - a) for 16-bit
-// storage -- the form the cell samplers compute with one mixed-precision
-// subtraction, so every path of an op gives the same bits.
+// storage -- the form the backprojectors and the 3D forward's direct and
+// xy-mode paths compute with one mixed-precision subtraction (the forward's
+// z-mode cells store half-differences instead: cone_fp_padded.cu).
 template <typename T>
 __device__ __forceinline__ float lerp_first(float a, float b, float t)
 {

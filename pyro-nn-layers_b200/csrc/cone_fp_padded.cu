@@ -21,6 +21,8 @@
 // does), so results match the direct path.
 #include <math_constants.h>
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "cone_ray.cuh"
 #include "internal.h"
@@ -44,10 +46,47 @@ __global__ void classify_views_kernel(const ConeFpView *__restrict__ views, int 
 
 // The eight taps of a trilinear cell, as (x0, x1) pairs in the order
 // (y0 z0), (y0 z1), (y1 z0), (y1 z1): two float4 for FP32, four 32-bit words
-// of two 16-bit values for BF16 / FP16 (x0 in the low half).
+// of two 16-bit values for BF16 / FP16 (x0 in the low half).  The 16-bit
+// cells hold the z0 taps and, in place of the z1 taps, the half-differences
+// (z1 - z0) / 2 rounded to the storage type (the halving keeps every FP16
+// difference finite); their z lerp z0 + (2t) ((z1 - z0) / 2) is one
+// mixed-precision FMA of two 16-bit operands (2t rounded to the storage type;
+// the product is exact in FP32) and one mixed-precision addition of the z0
+// tap (sm_100 fma.f32.f16 / add.f32.f16 and the bf16 forms): two instructions
+// per lerp instead of three (widen, mixed subtraction, FMA), measured on the
+// 512^3 forward at 96.8 -> 90.0 ms with the same error against the FP64 oracle
+// (2.65e-4 relative L2: FP16 storage's own rounding dominates).  The weight's
+// rounding (2^-12 relative for FP16) and the difference's are the only
+// departures from FP32 interpolation of the stored taps.
 struct alignas(16) CellF32 {
     float4 y0, y1;  // (x0 z0, x1 z0, x0 z1, x1 z1) at y0, then at y1
 };
+
+// z0 + t2 * hd for the z0 tap in word `a` and the half-difference in word
+// `d` (the half selected by HI) and t2 = 2t in the storage type
+template <bool BF16, bool HI>
+__device__ __forceinline__ float lerp_half_diff(unsigned a, unsigned d, unsigned short t2)
+{
+    float p, z;
+    if (BF16) {
+        if (HI) {
+            asm("{.reg .b16 l, h; mov.b32 {l, h}, %2; fma.rn.f32.bf16 %0, %1, h, %3;}" : "=f"(p) : "h"(t2), "r"(d), "f"(0.0f));
+            asm("{.reg .b16 l, h; mov.b32 {l, h}, %1; add.rn.f32.bf16 %0, h, %2;}" : "=f"(z) : "r"(a), "f"(p));
+        } else {
+            asm("{.reg .b16 l, h; mov.b32 {l, h}, %2; fma.rn.f32.bf16 %0, %1, l, %3;}" : "=f"(p) : "h"(t2), "r"(d), "f"(0.0f));
+            asm("{.reg .b16 l, h; mov.b32 {l, h}, %1; add.rn.f32.bf16 %0, l, %2;}" : "=f"(z) : "r"(a), "f"(p));
+        }
+    } else {
+        if (HI) {
+            asm("{.reg .b16 l, h; mov.b32 {l, h}, %2; fma.rn.f32.f16 %0, %1, h, %3;}" : "=f"(p) : "h"(t2), "r"(d), "f"(0.0f));
+            asm("{.reg .b16 l, h; mov.b32 {l, h}, %1; add.rn.f32.f16 %0, h, %2;}" : "=f"(z) : "r"(a), "f"(p));
+        } else {
+            asm("{.reg .b16 l, h; mov.b32 {l, h}, %2; fma.rn.f32.f16 %0, %1, l, %3;}" : "=f"(p) : "h"(t2), "r"(d), "f"(0.0f));
+            asm("{.reg .b16 l, h; mov.b32 {l, h}, %1; add.rn.f32.f16 %0, l, %2;}" : "=f"(z) : "r"(a), "f"(p));
+        }
+    }
+    return z;
+}
 
 template <typename T>
 struct Cell;
@@ -75,51 +114,44 @@ struct Cell<float> {
         return c;
     }
 };
-template <>
-struct Cell<__nv_bfloat16> {
+// the 16-bit cells: words (z0 taps at y0, half-differences at y0, z0 taps
+// at y1, half-differences at y1)
+template <typename T16>
+struct Cell16 {
+    static constexpr bool BF16 = std::is_same<T16, __nv_bfloat16>::value;
     using type = uint4;
-    // z lerps as a + t (b - a): the z0 tap a widened, b - a in one
-    // mixed-precision subtraction (sm_100 sub.f32.bf16), the FMA in FP32
     __device__ static void zlerp(const uint4 *c, float t, float (&z)[4])
     {
         const uint4 w = __ldg(c);
-        const float a0 = __uint_as_float(w.x << 16), a1 = __uint_as_float(w.x & 0xFFFF0000u);
-        const float a2 = __uint_as_float(w.z << 16), a3 = __uint_as_float(w.z & 0xFFFF0000u);
-        z[0] = fmaf(t, sub_f32_bf16<false>(w.y, a0), a0), z[1] = fmaf(t, sub_f32_bf16<true>(w.y, a1), a1);
-        z[2] = fmaf(t, sub_f32_bf16<false>(w.w, a2), a2), z[3] = fmaf(t, sub_f32_bf16<true>(w.w, a3), a3);
+        unsigned short t2;
+        if (BF16)
+            asm("cvt.rn.bf16.f32 %0, %1;" : "=h"(t2) : "f"(t + t));
+        else
+            asm("cvt.rn.f16.f32 %0, %1;" : "=h"(t2) : "f"(t + t));
+        z[0] = lerp_half_diff<BF16, false>(w.x, w.y, t2), z[1] = lerp_half_diff<BF16, true>(w.x, w.y, t2);
+        z[2] = lerp_half_diff<BF16, false>(w.z, w.w, t2), z[3] = lerp_half_diff<BF16, true>(w.z, w.w, t2);
     }
-    __device__ static uint4 make(const __nv_bfloat16 (&v)[8])
+    __device__ static unsigned short bits(__half v) { return __half_as_ushort(v); }
+    __device__ static unsigned short bits(__nv_bfloat16 v) { return __bfloat16_as_ushort(v); }
+    __device__ static unsigned short half_diff(T16 z1, T16 z0)
     {
-        unsigned w[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-            w[k] = (unsigned)__bfloat16_as_ushort(v[2 * k]) | ((unsigned)__bfloat16_as_ushort(v[2 * k + 1]) << 16);
-        return make_uint4(w[0], w[1], w[2], w[3]);
+        // (z1 - z0) / 2: exact in FP32, one rounding to the storage type
+        return bits(T16(0.5f * ((float)z1 - (float)z0)));
+    }
+    __device__ static uint4 make(const T16 (&v)[8])
+    {
+        const unsigned w0 = (unsigned)bits(v[0]) | ((unsigned)bits(v[1]) << 16);
+        const unsigned w1 = (unsigned)half_diff(v[2], v[0]) | ((unsigned)half_diff(v[3], v[1]) << 16);
+        const unsigned w2 = (unsigned)bits(v[4]) | ((unsigned)bits(v[5]) << 16);
+        const unsigned w3 = (unsigned)half_diff(v[6], v[4]) | ((unsigned)half_diff(v[7], v[5]) << 16);
+        return make_uint4(w0, w1, w2, w3);
     }
 };
 template <>
-struct Cell<__half> {
-    using type = uint4;
-    // z lerps as a + t (b - a): the z0 tap a widened, b - a in one
-    // mixed-precision subtraction (sm_100 sub.f32.f16), the FMA in FP32
-    __device__ static void zlerp(const uint4 *c, float t, float (&z)[4])
-    {
-        const uint4 w = __ldg(c);
-        const float a0 = __half2float(__ushort_as_half((unsigned short)(w.x & 0xFFFFu)));
-        const float a1 = __half2float(__ushort_as_half((unsigned short)(w.x >> 16)));
-        const float a2 = __half2float(__ushort_as_half((unsigned short)(w.z & 0xFFFFu)));
-        const float a3 = __half2float(__ushort_as_half((unsigned short)(w.z >> 16)));
-        z[0] = fmaf(t, sub_f32_f16<false>(w.y, a0), a0), z[1] = fmaf(t, sub_f32_f16<true>(w.y, a1), a1);
-        z[2] = fmaf(t, sub_f32_f16<false>(w.w, a2), a2), z[3] = fmaf(t, sub_f32_f16<true>(w.w, a3), a3);
-    }
-    __device__ static uint4 make(const __half (&v)[8])
-    {
-        unsigned w[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-            w[k] = (unsigned)__half_as_ushort(v[2 * k]) | ((unsigned)__half_as_ushort(v[2 * k + 1]) << 16);
-        return make_uint4(w[0], w[1], w[2], w[3]);
-    }
+struct Cell<__nv_bfloat16> : Cell16<__nv_bfloat16> {
+};
+template <>
+struct Cell<__half> : Cell16<__half> {
 };
 // z-fastest cell copy: element [xc][yc][zc], xc in [0, X+1], yc in [0, Y+1],
 // zc in [0, Z+1], holds the cell whose low corner is voxel (xc-1, yc-1, zc-1)

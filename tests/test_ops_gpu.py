@@ -157,7 +157,9 @@ def test_cone_projection_vs_oracle(cuda, dtype, hw):
     x = t(vol, cuda, dtype)
     out = pl.cone_projection3d(x, geo.detector_shape, *geo.args(), hardware_interp=hw, out_dtype=torch.float32)
     ref = oracle.cone_projection3d(rounded(x), geo.detector_shape, *geo.args(), hardware_interp=hw)
-    tol = 5e-4 if hw else 2e-5
+    # BF16 cells interpolate along z with the weight and the half-difference
+    # of the taps rounded to BF16 (measured 2.3e-5 here; FP16 stays within 2e-5)
+    tol = 5e-4 if hw else (5e-5 if dtype == torch.bfloat16 else 2e-5)
     assert rel_l2(out.cpu().numpy(), ref) < tol
 
 
