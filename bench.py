@@ -64,17 +64,17 @@ PHANTOM_ELLIPSOIDS = 32
 # (profiles/dram_cone512.md), keyed by (workload, volume storage, sinogram
 # storage, hardware_interp)
 NCU_DRAM_BYTES = {
-    ("cone512", "fp16", "fp16", False): 37.91e9 + 0.573e9,
+    ("cone512", "fp16", "fp16", False): 38.485e9 + 0.573e9,
 }
 # ncu counters of the forward kernel (profiles/cone_fp_padded_kernel_cone256_fp16.md,
 # a --set full capture at 256^3): issue activity, and L2 -> SM bytes per ray
 # sample scaled to a 512^3 launch by its sample count
 NCU_FORWARD_COUNTERS = {
     ("cone512", "fp16", "fp16", False): {
-        "issue_active": 0.829, "lanes_active_per_warp_instruction": 26.95,
-        "thread_instructions_per_sample": 46.7, "lts2xbar_bytes_per_sample_256": 11.0,
-        "source": "profiles/cone_fp_padded_kernel_cone256_fp16.md (256^3 capture; L2 -> SM bytes scale with "
-                  "the samples)"},
+        "issue_active": 0.829, "lanes_active_per_warp_instruction": 26.97,
+        "thread_instructions_per_sample": 44.7, "lts2xbar_bytes_per_sample_256": 11.0,
+        "source": "profiles/cone_fp_padded_kernel_cone256_fp16.md (256^3 capture; L2 -> SM bytes per sample "
+                  "from the earlier full capture, scaling with the samples)"},
 }
 # kernels of ours launched per fwd+back step (geometry preparation, view
 # classification, the two volume copies, forward; preparation, backprojection)
