@@ -35,7 +35,9 @@ constexpr int PB_X = 32;
 constexpr int PB_Y = 8;
 constexpr int PAD_TILE = 32;
 // workspace header words (after the error flag) set by classify_views_kernel
-enum { FLAG_NEED_XY = 1, FLAG_NEED_Z = 2 };
+// (FLAG_WIDE: a 16-bit input holds magnitudes whose differences may not fit
+// the storage type, so the cells take the FP32 y and x lerps)
+enum { FLAG_NEED_XY = 1, FLAG_NEED_Z = 2, FLAG_WIDE = 3 };
 
 __global__ void classify_views_kernel(const ConeFpView *__restrict__ views, int n, unsigned *__restrict__ flags)
 {
@@ -49,15 +51,15 @@ __global__ void classify_views_kernel(const ConeFpView *__restrict__ views, int 
 // of two 16-bit values for BF16 / FP16 (x0 in the low half).  The 16-bit
 // cells hold the z0 taps and, in place of the z1 taps, the half-differences
 // (z1 - z0) / 2 rounded to the storage type (the halving keeps every FP16
-// difference finite); their z lerp z0 + (2t) ((z1 - z0) / 2) is one
-// mixed-precision FMA of two 16-bit operands (2t rounded to the storage type;
-// the product is exact in FP32) and one mixed-precision addition of the z0
-// tap (sm_100 fma.f32.f16 / add.f32.f16 and the bf16 forms): two instructions
-// per lerp instead of three (widen, mixed subtraction, FMA), measured on the
-// 512^3 forward at 96.8 -> 90.0 ms with the same error against the FP64 oracle
-// (2.65e-4 relative L2: FP16 storage's own rounding dominates).  The weight's
-// rounding (2^-12 relative for FP16) and the difference's are the only
-// departures from FP32 interpolation of the stored taps.
+// difference finite).  Their z lerp z0 + (2t) ((z1 - z0) / 2) takes 16-bit
+// operands only: as one mixed-precision FMA and one mixed-precision addition
+// of the z0 tap (sm_100 fma.f32.f16 / add.f32.f16, bf16 alike), or, in the
+// packed form used unless the input's range forbids it, as a packed FMA on
+// the (x0, x1) pair, followed by the pair's y lerp in packed form and the x
+// lerp in FP32 (trilinear_packed).  Roundings to the storage type happen only
+// where neighbouring taps differ: the 512^3 forward's error against the FP64
+// oracle stays the storage rounding's (FP16 2.65e-4), measured at 96.8 ms
+// (widened taps, FP32 lerps) -> 90.0 ms (mixed z lerps) -> 83.0 ms (packed).
 struct alignas(16) CellF32 {
     float4 y0, y1;  // (x0 z0, x1 z0, x0 z1, x1 z1) at y0, then at y1
 };
@@ -106,6 +108,12 @@ struct Cell<float> {
         z[0] = lerp_ref(v[0], v[2], t), z[1] = lerp_ref(v[1], v[3], t);
         z[2] = lerp_ref(v[4], v[6], t), z[3] = lerp_ref(v[5], v[7], t);
     }
+    __device__ static float trilinear(const CellF32 *c, float tz, float ty, float tx)
+    {
+        float zl[4];
+        zlerp(c, tz, zl);
+        return lerp_ref(lerp_ref(zl[0], zl[2], ty), lerp_ref(zl[1], zl[3], ty), tx);
+    }
     __device__ static CellF32 make(const float (&v)[8])
     {
         CellF32 c;
@@ -131,6 +139,44 @@ struct Cell16 {
         z[0] = lerp_half_diff<BF16, false>(w.x, w.y, t2), z[1] = lerp_half_diff<BF16, true>(w.x, w.y, t2);
         z[2] = lerp_half_diff<BF16, false>(w.z, w.w, t2), z[3] = lerp_half_diff<BF16, true>(w.z, w.w, t2);
     }
+    // FP32 y and x lerps of the four z lerps (inputs of any magnitude)
+    __device__ static float trilinear(const uint4 *c, float tz, float ty, float tx)
+    {
+        float zl[4];
+        zlerp(c, tz, zl);
+        return lerp_ref(lerp_ref(zl[0], zl[2], ty), lerp_ref(zl[1], zl[3], ty), tx);
+    }
+    // Packed: the z lerps of the (x0, x1) pairs at y0 and at y1 as two FMAs
+    // on pairs of 16-bit values (z0 + (2t) hd, one rounding each), the y lerp
+    // of the pair as a packed difference and FMA, the x lerp in FP32 on the
+    // pair widened (one widening, one mixed-precision subtraction, one FMA):
+    // 11 instructions for the seven lerps instead of 16.  Differences of the
+    // interpolated pair must fit the storage type: used when every input
+    // magnitude is below Wide16<T16>::limit (FLAG_WIDE clear).
+    __device__ static float trilinear_packed(const uint4 *c, float tz, float ty, float tx)
+    {
+        const uint4 w = __ldg(c);
+        unsigned tz2, ty2, zy0, zy1, dy, yv;
+        if (BF16) {
+            asm("cvt.rn.bf16x2.f32 %0, %1, %1;" : "=r"(tz2) : "f"(tz + tz));
+            asm("cvt.rn.bf16x2.f32 %0, %1, %1;" : "=r"(ty2) : "f"(ty));
+            asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(zy0) : "r"(tz2), "r"(w.y), "r"(w.x));
+            asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(zy1) : "r"(tz2), "r"(w.w), "r"(w.z));
+            asm("sub.rn.bf16x2 %0, %1, %2;" : "=r"(dy) : "r"(zy1), "r"(zy0));
+            asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(yv) : "r"(ty2), "r"(dy), "r"(zy0));
+            const float lo = __uint_as_float(yv << 16);
+            return fmaf(tx, sub_f32_bf16<true>(yv, lo), lo);
+        } else {
+            asm("cvt.rn.f16x2.f32 %0, %1, %1;" : "=r"(tz2) : "f"(tz + tz));
+            asm("cvt.rn.f16x2.f32 %0, %1, %1;" : "=r"(ty2) : "f"(ty));
+            asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(zy0) : "r"(tz2), "r"(w.y), "r"(w.x));
+            asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(zy1) : "r"(tz2), "r"(w.w), "r"(w.z));
+            asm("sub.rn.f16x2 %0, %1, %2;" : "=r"(dy) : "r"(zy1), "r"(zy0));
+            asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(yv) : "r"(ty2), "r"(dy), "r"(zy0));
+            const float lo = __half2float(__ushort_as_half((unsigned short)(yv & 0xFFFFu)));
+            return fmaf(tx, sub_f32_f16<true>(yv, lo), lo);
+        }
+    }
     __device__ static unsigned short bits(__half v) { return __half_as_ushort(v); }
     __device__ static unsigned short bits(__nv_bfloat16 v) { return __bfloat16_as_ushort(v); }
     __device__ static unsigned short half_diff(T16 z1, T16 z0)
@@ -153,6 +199,22 @@ struct Cell<__nv_bfloat16> : Cell16<__nv_bfloat16> {
 template <>
 struct Cell<__half> : Cell16<__half> {
 };
+// Magnitudes above which the packed lerps' differences of two interpolated
+// 16-bit values could leave the storage type's range (FP16: 2 x 32752 = 65504,
+// its largest finite value); FP32 input never takes the packed lerps.
+template <typename T>
+struct Wide16 {
+    __device__ static bool exceeds(T) { return false; }
+};
+template <>
+struct Wide16<__half> {
+    __device__ static bool exceeds(__half v) { return fabsf(__half2float(v)) > 32752.0f; }
+};
+template <>
+struct Wide16<__nv_bfloat16> {
+    __device__ static bool exceeds(__nv_bfloat16 v) { return fabsf(__bfloat162float(v)) > 8.5e37f; }
+};
+
 // z-fastest cell copy: element [xc][yc][zc], xc in [0, X+1], yc in [0, Y+1],
 // zc in [0, Z+1], holds the cell whose low corner is voxel (xc-1, yc-1, zc-1)
 // (V zero outside the volume), i.e. the taps of every floor in [-1, N].
@@ -161,10 +223,11 @@ struct Cell<__half> : Cell16<__half> {
 template <typename T>
 __global__ void __launch_bounds__(PAD_TILE *8) pad_cells_kernel(const T *__restrict__ src,
                                                                  typename Cell<T>::type *__restrict__ dst, int X,
-                                                                 int Y, int Z, const unsigned *__restrict__ flags)
+                                                                 int Y, int Z, unsigned *__restrict__ flags)
 {
     if (!flags[FLAG_NEED_Z]) return;
     __shared__ T tile[2][PAD_TILE + 1][PAD_TILE + 2];  // [y - (yc-1)][z - (zc0-1)][x - (xc0-1)]
+    bool wide = false;
     const int Yc = Y + 2, Zc = Z + 2;
     const int xc0 = blockIdx.x * PAD_TILE, yc = blockIdx.y, zc0 = blockIdx.z * PAD_TILE;
     for (int rr = threadIdx.y; rr < 2 * (PAD_TILE + 1); rr += 8) {
@@ -175,10 +238,11 @@ __global__ void __launch_bounds__(PAD_TILE *8) pad_cells_kernel(const T *__restr
             const int x = xc0 - 1 + c;
             T v = T(0.0f);
             if (yz_in && x >= 0 && x < X) v = src[((size_t)z * Y + y) * X + x];
+            wide |= Wide16<T>::exceeds(v);
             tile[dy][r][c] = v;
         }
     }
-    __syncthreads();
+    if (__syncthreads_or(wide) && threadIdx.x == 0 && threadIdx.y == 0) atomicOr(&flags[FLAG_WIDE], 1u);
     const int tz = threadIdx.x, zc = zc0 + tz;
     if (zc >= Zc) return;
     for (int c = threadIdx.y; c < PAD_TILE; c += 8) {
@@ -282,7 +346,7 @@ __device__ __forceinline__ bool march_inside(const ConeRay &r, int X, int Y, int
 // Trilinear interpolation from the cell copy: one cell load gives the eight
 // taps.  `origin` points at the cell of floor (0, 0, 0); the floor bias of
 // the three FloorFrac bit patterns is folded into one per-sampler offset.
-template <typename T>
+template <typename T, bool PACKED>
 struct CellSampler {
     const typename Cell<T>::type *origin;
     unsigned s_y, s_x;  // cell strides of y and x (z is fastest)
@@ -299,21 +363,38 @@ struct CellSampler {
         const FloorFrac fx = floor_frac(x), fy = floor_frac(y), fz = floor_frac(z);
         const unsigned idx = (unsigned)fx.bits * s_x + (unsigned)fy.bits * s_y + (unsigned)fz.bits + bias;
         // the reference's order: lerp in z, then y, then x
-        float zl[4];
-        Cell<T>::zlerp(origin + (int)idx, fz.f, zl);
-        return lerp_ref(lerp_ref(zl[0], zl[2], fy.f), lerp_ref(zl[1], zl[3], fy.f), fx.f);
+        if constexpr (PACKED)
+            return Cell<T>::trilinear_packed(origin + (int)idx, fz.f, fy.f, fx.f);
+        else
+            return Cell<T>::trilinear(origin + (int)idx, fz.f, fy.f, fx.f);
     }
 };
 
-template <typename T>
+template <typename T, bool PACKED>
 struct ClampedCellSampler {
-    CellSampler<T> s;
+    CellSampler<T, PACKED> s;
     float xmax, ymax, zmax;
     __device__ __forceinline__ float operator()(float x, float y, float z) const
     {
         return s(fminf(fmaxf(x, -1.0f), xmax), fminf(fmaxf(y, -1.0f), ymax), fminf(fmaxf(z, -1.0f), zmax));
     }
 };
+
+// The march of one z-mode ray over the cell copy.
+template <typename T, bool PACKED>
+__device__ __forceinline__ float march_cells(const ConeRay &ray, float step, bool inside,
+                                             const typename Cell<T>::type *cells, int Y, int Z, float xmax,
+                                             float ymax, float zmax)
+{
+    const int Yc = Y + 2, Zc = Z + 2;
+    const CellSampler<T, PACKED> s(cells + (Yc + 1) * Zc + 1, Zc, Yc * Zc);
+    const int n = inside ? exact_sample_count(ray, step) : -1;
+    // eight samples per iteration for 16-bit cells, four for the 32-byte
+    // FP32 cells (whose loads need twice the registers)
+    return n > 0    ? march_counted<sizeof(T) == 4 ? 4 : 8>(ray, n, step, s)
+           : inside ? march_x2(ray, step, s)
+                    : march_x2(ray, step, ClampedCellSampler<T, PACKED>{s, xmax, ymax, zmax});
+}
 
 // Grid: one dimension, ray_block_count blocks in ray_block order (four
 // blocks of 256 threads per 32 x 32 ray tile, neighbouring views of a tile
@@ -328,7 +409,7 @@ __global__ void __launch_bounds__(PB_X *PB_Y, 4)
                           const typename Cell<T>::type *__restrict__ cells, Tout *__restrict__ sino,
                           const ConeFpView *__restrict__ views, const float *__restrict__ step_ptr,
                           const float *__restrict__ spacing_ptr, int X, int Y, int Z, int W, int H, int n_proj,
-                          int geom_batch, int b)
+                          int geom_batch, int b, const unsigned *__restrict__ flags)
 {
     __shared__ float out_tile[PB_Y][PB_X + 1];
     const RayBlock rb = ray_block(blockIdx.x, W, H, n_proj);
@@ -346,6 +427,8 @@ __global__ void __launch_bounds__(PB_X *PB_Y, 4)
     }
     const bool live = u < W && v < H;
     const float step = step_ptr[g];
+    // 16-bit cells take the packed lerps unless the input's range forbids them
+    const bool packed = sizeof(T) == 2 && !flags[FLAG_WIDE];
     float pixel = 0.0f;
     if (live) {
         const ConeRay ray = cone_ray_setup(view, u, v, X, Y, Z, 0.0, step, spacing_ptr[g * 3 + 2],
@@ -354,14 +437,10 @@ __global__ void __launch_bounds__(PB_X *PB_Y, 4)
         const float xmax = (float)X + 0.999f, ymax = (float)Y + 0.999f, zmax = (float)Z + 0.999f;
         const int Xp = X + 3, Yp = Y + 3;
         if (zmode) {
-            const int Yc = Y + 2, Zc = Z + 2;
-            const CellSampler<T> s(cells + (Yc + 1) * Zc + 1, Zc, Yc * Zc);
-            const int n = inside ? exact_sample_count(ray, step) : -1;
-            // eight samples per iteration for 16-bit cells, four for the
-            // 32-byte FP32 cells (whose loads need twice the registers)
-            pixel = n > 0    ? march_counted<sizeof(T) == 4 ? 4 : 8>(ray, n, step, s)
-                    : inside ? march_x2(ray, step, s)
-                             : march_x2(ray, step, ClampedCellSampler<T>{s, xmax, ymax, zmax});
+            if (packed)
+                pixel = march_cells<T, sizeof(T) == 2>(ray, step, inside, cells, Y, Z, xmax, ymax, zmax);
+            else
+                pixel = march_cells<T, false>(ray, step, inside, cells, Y, Z, xmax, ymax, zmax);
         } else {
             // rays mostly along x -> y-fastest copy
             const double cr0 = view.inv_ar[2] + 0.5 * (W - 1) * view.inv_ar[0] + 0.5 * (H - 1) * view.inv_ar[1];
@@ -421,7 +500,8 @@ cudaError_t launch_typed(const void *volume, void *sinogram, const Dims3D &d, co
         pad_cells_kernel<Tin><<<cgrid, pblock, 0, stream>>>(src, cells, d.vol_x, d.vol_y, d.vol_z, flags);
         cone_fp_padded_kernel<Tin, Tout><<<grid, block, 0, stream>>>(xfast, yfast, cells, (Tout *)sinogram, views,
                                                                      step, spacing, d.vol_x, d.vol_y, d.vol_z,
-                                                                     d.det_w, d.det_h, d.n_proj, d.geom_batch, b);
+                                                                     d.det_w, d.det_h, d.n_proj, d.geom_batch, b,
+                                                                     flags);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }

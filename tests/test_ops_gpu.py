@@ -34,6 +34,10 @@ pytestmark = pytest.mark.gpu
 
 DTYPES = [torch.float32, torch.bfloat16, torch.float16]
 OUT_TOL = {torch.float32: 0.0, torch.bfloat16: 4e-3, torch.float16: 6e-4}
+# the 3D forward's 16-bit cells interpolate in the storage type (z lerps of
+# the z0 taps and the stored half-differences, y lerp of the pair, one
+# rounding each; measured on these phantoms: FP16 1.4e-5, BF16 1.1e-4)
+CONE_FWD_TOL = {torch.float32: 2e-5, torch.float16: 2e-5, torch.bfloat16: 2e-4}
 
 
 def t(a, dev, dtype=torch.float32):
@@ -157,9 +161,7 @@ def test_cone_projection_vs_oracle(cuda, dtype, hw):
     x = t(vol, cuda, dtype)
     out = pl.cone_projection3d(x, geo.detector_shape, *geo.args(), hardware_interp=hw, out_dtype=torch.float32)
     ref = oracle.cone_projection3d(rounded(x), geo.detector_shape, *geo.args(), hardware_interp=hw)
-    # BF16 cells interpolate along z with the weight and the half-difference
-    # of the taps rounded to BF16 (measured 2.3e-5 here; FP16 stays within 2e-5)
-    tol = 5e-4 if hw else (5e-5 if dtype == torch.bfloat16 else 2e-5)
+    tol = 5e-4 if hw else CONE_FWD_TOL[dtype]
     assert rel_l2(out.cpu().numpy(), ref) < tol
 
 
@@ -454,6 +456,22 @@ def test_cone_projection_non_circular_views(cuda, dtype):
     x = t(vol, cuda, dtype)
     out = pl.cone_projection3d(x, geo.detector_shape, *args, out_dtype=torch.float32)
     ref = oracle.cone_projection3d(rounded(x), geo.detector_shape, *args)
+    assert rel_l2(out.cpu().numpy(), ref) < CONE_FWD_TOL[dtype]
+
+
+def test_cone_projection_wide_fp16_range(cuda):
+    """FP16 inputs whose magnitudes could overflow FP16 in the packed lerps'
+    differences (above 32752) take FP32 y and x lerps: the cell copy flags
+    them, and the result matches the oracle as closely as a normal-range
+    input's.  (The BF16 bound, 8.5e37, lies beyond what FP32 sums of a ray can
+    hold anyway.)"""
+    geo = _cone_geo()
+    vol = phantoms.ellipsoid_phantom_3d(geo.volume_shape, geo.volume_spacing, seed=5, n=6)[0][None]
+    x = t(vol / vol.max() * 40000.0, cuda, torch.float16)
+    x[0, 3, 4, 5] = -40000.0  # a negative extreme beside positive ones
+    out = pl.cone_projection3d(x, geo.detector_shape, *geo.args(), out_dtype=torch.float32)
+    ref = oracle.cone_projection3d(rounded(x), geo.detector_shape, *geo.args())
+    assert torch.isfinite(out).all()
     assert rel_l2(out.cpu().numpy(), ref) < 2e-5
 
 

@@ -159,7 +159,7 @@ def test_config4_gradient_against_central_differences(cuda):
 
 
 def test_config3_cone512_headline_samples(cuda):
-    """The headline geometry at full size with FP16 storage (FP32 arithmetic):
+    """The headline geometry at full size with FP16 storage (FP32 sums):
     views 0 and 97 of the forward projection and z-slices 254..257 of the
     backprojection against the oracle on the same FP16-rounded inputs."""
     geo = geometry.ConeBeam3D((512, 512, 512), (0.5, 0.5, 0.5), (768, 1024), (1.0, 1.0), 360, 750.0, 1200.0,
