@@ -362,8 +362,8 @@ int pyronn_cone_projection3d(const void *volume, void *sinogram, int in_dtype, i
     ConeFpView *views = (ConeFpView *)((char *)workspace + WS_HEADER);
     cudaError_t e = cudaMemsetAsync(workspace, 0, WS_HEADER, s);
     if (e != cudaSuccess) return cuda_fail(e, "cone_projection3d: workspace header");
-    e = launch_cone_fp_prepare(projection_matrices, volume_spacing, volume_origin, geom_batch, n_proj,
-                                           views, s);
+    e = launch_cone_fp_prepare(projection_matrices, volume_spacing, volume_origin, geom_batch, n_proj, vol_x, vol_y,
+                               vol_z, views, s);
     if (e != cudaSuccess) return cuda_fail(e, "cone_projection3d: geometry preparation");
     if (!hardware_interp) {
         if (cone_fp_padded_supported(d)) {
@@ -478,7 +478,8 @@ int pyronn_cone_backprojection3d_matched(const void *sinogram, float *volume, in
     ConeFpView *views = (ConeFpView *)((char *)workspace + WS_HEADER);
     cudaError_t e = cudaMemsetAsync(workspace, 0, WS_HEADER, s);
     if (e == cudaSuccess)
-        e = launch_cone_fp_prepare(projection_matrices, volume_spacing, volume_origin, geom_batch, n_proj, views, s);
+        e = launch_cone_fp_prepare(projection_matrices, volume_spacing, volume_origin, geom_batch, n_proj, vol_x,
+                                   vol_y, vol_z, views, s);
     if (e == cudaSuccess) e = launch_cone_scatter(sinogram, volume, in_dtype, d, views, step_size, volume_spacing, s);
     if (e != cudaSuccess) return cuda_fail(e, name);
     return ok();

@@ -85,10 +85,14 @@ __global__ void __launch_bounds__(FP_BLOCK_X *FP_BLOCK_Y)
     if (u >= W || v >= H) return;
     const int g = geom_batch == 1 ? 0 : b;
     const float step = step_ptr[g];
-    const ConeRay ray = cone_ray_setup(views[(size_t)g * n_proj + p], u, v, X, Y, Z, HW ? -0.5 : 0.0, step,
-                                       spacing_ptr[g * 3 + 2], spacing_ptr[g * 3 + 1], spacing_ptr[g * 3 + 0]);
-    const Sampler<T, HW> sample{vol + (size_t)b * X * Y * Z, tex, X, Y, Z};
-    const float pixel = cone_ray_march<false>(ray, step, sample);
+    const ConeFpView &view = views[(size_t)g * n_proj + p];
+    float pixel = 0.0f;
+    if (in_footprint(view, u, v)) {
+        const ConeRay ray = cone_ray_setup(view, u, v, X, Y, Z, HW ? -0.5 : 0.0, step, spacing_ptr[g * 3 + 2],
+                                           spacing_ptr[g * 3 + 1], spacing_ptr[g * 3 + 0]);
+        const Sampler<T, HW> sample{vol + (size_t)b * X * Y * Z, tex, X, Y, Z};
+        pixel = cone_ray_march<false>(ray, step, sample);
+    }
     store_from_float(sino + (((size_t)b * n_proj + p) * H + v) * (size_t)W + u, pixel);
 }
 
@@ -115,11 +119,15 @@ __global__ void __launch_bounds__(256)
     if (u >= W || v >= H) return;
     const int g = geom_batch == 1 ? 0 : b;
     const float step = step_ptr[g];
-    const ConeRay ray = cone_ray_setup(views[(size_t)g * n_proj + rb.p], u, v, X, Y, Z, -0.5, step,
-                                       spacing_ptr[g * 3 + 2], spacing_ptr[g * 3 + 1], spacing_ptr[g * 3 + 0]);
-    const TexSampler s{tex};
-    const int n = exact_sample_count(ray, step);
-    const float pixel = n > 0 ? march_counted_x2(ray, n, step, s) : march_x2(ray, step, s);
+    const ConeFpView &view = views[(size_t)g * n_proj + rb.p];
+    float pixel = 0.0f;
+    if (in_footprint(view, u, v)) {
+        const ConeRay ray = cone_ray_setup(view, u, v, X, Y, Z, -0.5, step, spacing_ptr[g * 3 + 2],
+                                           spacing_ptr[g * 3 + 1], spacing_ptr[g * 3 + 0]);
+        const TexSampler s{tex};
+        const int n = exact_sample_count(ray, step);
+        pixel = n > 0 ? march_counted_x2(ray, n, step, s) : march_x2(ray, step, s);
+    }
     store_from_float(sino + (((size_t)b * n_proj + rb.p) * H + v) * (size_t)W + u, pixel);
 }
 

@@ -430,7 +430,7 @@ __global__ void __launch_bounds__(PB_X *PB_Y, 4)
     // 16-bit cells take the packed lerps unless the input's range forbids them
     const bool packed = sizeof(T) == 2 && !flags[FLAG_WIDE];
     float pixel = 0.0f;
-    if (live) {
+    if (live && in_footprint(view, u, v)) {
         const ConeRay ray = cone_ray_setup(view, u, v, X, Y, Z, 0.0, step, spacing_ptr[g * 3 + 2],
                                            spacing_ptr[g * 3 + 1], spacing_ptr[g * 3 + 0]);
         const bool inside = march_inside(ray, X, Y, Z);

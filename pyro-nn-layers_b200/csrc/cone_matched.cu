@@ -62,6 +62,7 @@ __global__ void __launch_bounds__(MB_X *MB_Y)
     if (y == 0.0f) return;
     const int g = geom_batch == 1 ? 0 : b;
     const float step = step_ptr[g];
+    if (!in_footprint(views[(size_t)g * n_proj + p], u, v)) return;
     const ConeRay ray = cone_ray_setup(views[(size_t)g * n_proj + p], u, v, X, Y, Z, 0.0, step,
                                        spacing_ptr[g * 3 + 2], spacing_ptr[g * 3 + 1], spacing_ptr[g * 3 + 0]);
     float *vol_b = vol + (size_t)b * Z * Y * X;

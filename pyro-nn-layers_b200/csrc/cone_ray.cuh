@@ -28,6 +28,15 @@ struct ConeRay {
     float mm_scale;    // |direction (.) spacing|: index length -> mm (:217-219)
 };
 
+// Whether detector pixel (u, v) lies in the view's footprint of the volume
+// box: rays outside it miss the box, so their set-up (FP64) is skipped and
+// their value is the miss's, 0.
+__device__ __forceinline__ bool in_footprint(const ConeFpView &view, int u, int v)
+{
+    const float fu = (float)u, fv = (float)v;
+    return fu >= view.foot[0] && fu <= view.foot[1] && fv >= view.foot[2] && fv <= view.foot[3];
+}
+
 __device__ __forceinline__ ConeRay cone_ray_setup(const ConeFpView &view, int u, int v, int X, int Y, int Z,
                                                   double lo, float step, float spx, float spy, float spz)
 {

@@ -6,6 +6,8 @@
 // cc/helper_headers/helper_geometry_cpu.h:30-43).  Here one thread per view
 // does it in FP64 on the stream: C = -M^-1 p4 is the right null vector of
 // P = [M | p4] already normalised to C[3] = 1, so no SVD is needed.
+#include <math_constants.h>
+
 #include "internal.h"
 
 namespace pyronn {
@@ -31,8 +33,8 @@ __device__ void invert3x3(const double *m, double *inv)
 
 // spacing/origin rows are in (z, y, x) order, as the reference op receives them
 __global__ void cone_fp_prepare_kernel(const float *__restrict__ P, const float *__restrict__ spacing,
-                                       const float *__restrict__ origin, int geom_batch, int n_proj,
-                                       ConeFpView *__restrict__ out)
+                                       const float *__restrict__ origin, int geom_batch, int n_proj, int X, int Y,
+                                       int Z, ConeFpView *__restrict__ out)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= geom_batch * n_proj) return;
@@ -50,6 +52,28 @@ __global__ void cone_fp_prepare_kernel(const float *__restrict__ P, const float 
         v.src[r] = (c - o[r]) / s[r];
         for (int k = 0; k < 3; ++k) v.inv_ar[3 * r + k] = inv[3 * r + k] / s[r];
     }
+    // footprint: the eight corners of the box [-0.5, N] (index space, the
+    // union of the software [0, N] and texture [-0.5, N - 0.5] boxes) through
+    // P; the box is convex and, with every corner on one side of the source,
+    // its image is the convex hull of the corners' images
+    double u0 = CUDART_INF, u1 = -CUDART_INF, v0 = CUDART_INF, v1 = -CUDART_INF;
+    int pos = 0, neg = 0;
+    for (int c = 0; c < 8; ++c) {
+        const double ix = (c & 1) ? (double)X : -0.5, iy = (c & 2) ? (double)Y : -0.5, iz = (c & 4) ? (double)Z : -0.5;
+        const double wx = o[0] + s[0] * ix, wy = o[1] + s[1] * iy, wz = o[2] + s[2] * iz;
+        const double hu = (double)p[0] * wx + (double)p[1] * wy + (double)p[2] * wz + (double)p[3];
+        const double hv = (double)p[4] * wx + (double)p[5] * wy + (double)p[6] * wz + (double)p[7];
+        const double hw = (double)p[8] * wx + (double)p[9] * wy + (double)p[10] * wz + (double)p[11];
+        pos += hw > 0.0;
+        neg += hw < 0.0;
+        const double cu = hu / hw, cv = hv / hw;
+        u0 = fmin(u0, cu), u1 = fmax(u1, cu), v0 = fmin(v0, cv), v1 = fmax(v1, cv);
+    }
+    const bool bounded = (pos == 8 || neg == 8) && isfinite(u0) && isfinite(u1) && isfinite(v0) && isfinite(v1);
+    v.foot[0] = bounded ? (float)(u0 - 2.0) : -CUDART_INF_F;
+    v.foot[1] = bounded ? (float)(u1 + 2.0) : CUDART_INF_F;
+    v.foot[2] = bounded ? (float)(v0 - 2.0) : -CUDART_INF_F;
+    v.foot[3] = bounded ? (float)(v1 + 2.0) : CUDART_INF_F;
     out[t] = v;
 }
 
@@ -78,10 +102,11 @@ __global__ void cone_bp_prepare_kernel(const float *__restrict__ P, const float 
 }  // namespace
 
 cudaError_t launch_cone_fp_prepare(const float *P, const float *spacing, const float *origin, int geom_batch,
-                                   int n_proj, ConeFpView *out, cudaStream_t stream)
+                                   int n_proj, int vol_x, int vol_y, int vol_z, ConeFpView *out, cudaStream_t stream)
 {
     const int n = geom_batch * n_proj;
-    cone_fp_prepare_kernel<<<(n + 127) / 128, 128, 0, stream>>>(P, spacing, origin, geom_batch, n_proj, out);
+    cone_fp_prepare_kernel<<<(n + 127) / 128, 128, 0, stream>>>(P, spacing, origin, geom_batch, n_proj, vol_x, vol_y,
+                                                                vol_z, out);
     return cudaGetLastError();
 }
 

@@ -15,6 +15,11 @@ namespace pyronn {
 struct ConeFpView {
     double inv_ar[9];
     double src[3];
+    // detector footprint of the volume box [-0.5, N] per axis, in pixel
+    // indices (u_min, u_max, v_min, v_max), widened by 2 pixels: a ray whose
+    // pixel lies outside misses the box; unbounded (+-inf) when the box's
+    // corners do not all lie on one side of the source
+    float foot[4];
 };
 
 // Per-view cone backprojection matrix in voxel-index space:
@@ -38,7 +43,7 @@ struct Dims3D {
 
 // geometry preparation (geometry.cu)
 cudaError_t launch_cone_fp_prepare(const float *P, const float *spacing, const float *origin, int geom_batch,
-                                   int n_proj, ConeFpView *out, cudaStream_t stream);
+                                   int n_proj, int vol_x, int vol_y, int vol_z, ConeFpView *out, cudaStream_t stream);
 cudaError_t launch_cone_bp_prepare(const float *P, const float *spacing, const float *origin, int geom_batch,
                                    int n_proj, ConeBpView *out, cudaStream_t stream);
 
