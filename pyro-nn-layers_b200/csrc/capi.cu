@@ -319,9 +319,13 @@ size_t pyronn_cone_projection3d_workspace_size(int batch, int vol_z, int vol_y, 
 size_t pyronn_cone_backprojection3d_workspace_size(int batch, int n_proj, int det_h, int det_w, int vol_z, int vol_y,
                                                    int vol_x, int in_dtype, int hardware_interp, int geom_batch)
 {
-    (void)batch, (void)det_h, (void)det_w, (void)vol_z, (void)vol_y, (void)vol_x, (void)hardware_interp;
     if (geom_batch <= 0 || n_proj <= 0 || !valid_dtype(in_dtype)) return 0;
-    return WS_HEADER + align_up((size_t)geom_batch * n_proj * sizeof(ConeBpView), 256);
+    const size_t views = WS_HEADER + align_up((size_t)geom_batch * n_proj * sizeof(ConeBpView), 256);
+    if (hardware_interp || batch <= 0 || det_h <= 0 || det_w <= 0) return views;
+    // 16-bit sinograms: room for the paired copy the TMA path reads (a
+    // workspace of `views` bytes alone is accepted, without the pairing)
+    const Dims3D d{batch, vol_z, vol_y, vol_x, n_proj, det_h, det_w, geom_batch};
+    return views + align_up(cone_bp_tma_paired_bytes(in_dtype, d), 256);
 }
 
 int pyronn_workspace_error(const void *workspace, void *stream, int *device_error)
@@ -405,8 +409,8 @@ int pyronn_cone_backprojection3d(const void *sinogram, void *volume, int in_dtyp
     int st = check_cone(name, sinogram, volume, in_dtype, out_dtype, d, volume_origin, volume_spacing, projection_matrices,
                         step_size, projection_multiplier);
     if (st) return st;
-    const size_t need = pyronn_cone_backprojection3d_workspace_size(batch, n_proj, det_h, det_w, vol_z, vol_y, vol_x,
-                                                                    in_dtype, hardware_interp, geom_batch);
+    // the views' part is required; the paired copy is used when it fits
+    const size_t need = WS_HEADER + align_up((size_t)geom_batch * n_proj * sizeof(ConeBpView), 256);
     if (!workspace || workspace_bytes < need)
         return fail(PYRONN_ERROR_WORKSPACE_TOO_SMALL, "%s: workspace of %zu bytes needed, %zu given", name, need,
                     workspace ? workspace_bytes : (size_t)0);
@@ -424,8 +428,12 @@ int pyronn_cone_backprojection3d(const void *sinogram, void *volume, int in_dtyp
     e = launch_cone_bp_prepare(projection_matrices, volume_spacing, volume_origin, geom_batch, n_proj, views, s);
     if (e != cudaSuccess) return cuda_fail(e, "cone_backprojection3d: geometry preparation");
     if (!hardware_interp) {
-        if (cone_bp_tma_supported(sinogram, in_dtype, d))
-            e = launch_cone_bp_tma(sinogram, volume, in_dtype, out_dtype, d, views, projection_multiplier, err, s);
+        if (cone_bp_tma_supported(sinogram, in_dtype, d)) {
+            const size_t pb = cone_bp_tma_paired_bytes(in_dtype, d);
+            void *paired = (pb > 0 && workspace_bytes >= need + pb) ? (char *)workspace + need : nullptr;
+            e = launch_cone_bp_tma(sinogram, volume, in_dtype, out_dtype, d, views, projection_multiplier, err,
+                                   paired, s);
+        }
         else
             e = launch_cone_bp(sinogram, volume, in_dtype, out_dtype, d, -1, views, projection_multiplier, 0, s);
         if (e != cudaSuccess) return cuda_fail(e, name);

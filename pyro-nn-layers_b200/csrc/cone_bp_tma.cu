@@ -16,6 +16,13 @@
 // bounded) for the two passes that can still have boxes in flight.  Its
 // voxels are stored, invalid: the error word says so.
 //
+// Given room in the workspace, a 16-bit sinogram is first copied into a
+// paired layout -- element u + 1 of a detector row holds taps u and u + 1 --
+// and the boxes stage those 32-bit pairs: a lerp along u is then one shared-
+// memory load instead of two, on the same taps with the same operations (the
+// same bits).  512^3 workload: backprojection 32.5 -> 31.8 ms, the pairing
+// pass (1.1 GB written) included.
+//
 // Exactness: the tap indices and weights are computed exactly as the direct
 // path computes them (floor of u/w, frac), only the texel source differs.  TMA
 // zero-fills out-of-range texels, which equals the reference's semantics for
@@ -50,6 +57,23 @@ constexpr int BP_K = 4;  // views per pass
 constexpr int BOX_W = 72;  // 72-element rows shift banks between rows (64 would alias them)
 constexpr int BOX_H = 24;
 constexpr int BOX_ELEMS = BOX_W * BOX_H;
+// Paired boxes (16-bit sinograms given a workspace for the paired copy):
+// 32-bit elements (tap u, tap u + 1), 68-word rows (4 banks of shift per row)
+constexpr int BOX_WP = 68;
+
+// The staged box of a sinogram type: element type, row length, TMA x
+// alignment (elements) and the paired copy's column offset (element u + 1
+// holds taps u and u + 1; element 0 holds a zero tap -1 and tap 0).
+template <typename T, bool PAIRED>
+struct BoxLayout {
+    using E = T;
+    static constexpr int W = BOX_W, ALIGN = 16 / (int)sizeof(T), OFF = 0;
+};
+template <typename T>
+struct BoxLayout<T, true> {
+    using E = unsigned;
+    static constexpr int W = BOX_WP, ALIGN = 4, OFF = 1;
+};
 
 enum ViewMode : int { MODE_SMEM = 0, MODE_GLOBAL = 1, MODE_SKIP = 2 };
 
@@ -85,6 +109,31 @@ __device__ __forceinline__ float smem_ulerp<__nv_bfloat16>(const __nv_bfloat16 *
     return fmaf(t, sub_f32_bf16<false>(__bfloat16_as_ushort(p[1]), a), a);
 }
 
+// the same lerp on a paired element: tap u in the low half, tap u + 1 in the
+// high half (the same operations, hence the same bits)
+template <typename T>
+__device__ __forceinline__ float pair_ulerp(unsigned w, float t);
+template <>
+__device__ __forceinline__ float pair_ulerp<__half>(unsigned w, float t)
+{
+    const float a = __half2float(__ushort_as_half((unsigned short)(w & 0xFFFFu)));
+    return fmaf(t, sub_f32_f16<true>(w, a), a);
+}
+template <>
+__device__ __forceinline__ float pair_ulerp<__nv_bfloat16>(unsigned w, float t)
+{
+    const float a = __uint_as_float(w << 16);
+    return fmaf(t, sub_f32_bf16<true>(w, a), a);
+}
+template <typename T, bool PAIRED>
+__device__ __forceinline__ float box_ulerp(const typename BoxLayout<T, PAIRED>::E *p, float t)
+{
+    if constexpr (PAIRED)
+        return pair_ulerp<T>(*p, t);  // 16-bit sinograms only
+    else
+        return smem_ulerp(p, t);
+}
+
 // tap rules of interp2D, cone_backprojector_3D_CudaKernel.cu.cc:55-82
 template <typename T>
 __device__ __forceinline__ float interp_global(const T *__restrict__ sino, float u, float v, unsigned view_base, int W,
@@ -107,13 +156,16 @@ __device__ __forceinline__ float interp_global(const T *__restrict__ sino, float
     return lerp_ref(lerp_first<T>(p00, p01, tx), lerp_first<T>(p10, p11, tx), ty);
 }
 
-template <typename T>
-struct TmaTraits {
-    static constexpr int ALIGN = 16 / (int)sizeof(T);  // TMA x alignment in elements
-};
+// Resident blocks per SM the kernel is compiled for: the paired layout runs
+// best at 4 (64 registers; 3 blocks with 80: 512^3 backprojection 31.8 vs
+// 32.6 ms), the unpaired at the compiler's choice (80 registers, 3 blocks for
+// 16-bit taps: 32.5 ms, against 33.1 ms forced to 4; 0 = no minimum)
+#ifndef PYRONN_BP_MIN_BLOCKS
+#define PYRONN_BP_MIN_BLOCKS(paired) ((paired) ? 4 : 0)
+#endif
 
 // Computes the metadata of one pass (warp 0 only): lane = k * 8 + corner.
-template <typename T>
+template <typename T, bool PAIRED>
 __device__ __forceinline__ void pass_meta(ViewMeta *meta, const ConeBpView *__restrict__ pv, int n_first, int n_proj,
                                           int i0, int j0, int k0, int W, int H)
 {
@@ -161,10 +213,15 @@ __device__ __forceinline__ void pass_meta(ViewMeta *meta, const ConeBpView *__re
             if (x_hi < 0 || y_hi < 0 || x_lo > W || y_lo > H) {
                 mode = MODE_SKIP;  // every tap outside the detector and past the quirk row/column
             } else {
-                const int a = TmaTraits<T>::ALIGN;
-                iu0 = (x_lo >= 0) ? (x_lo / a) * a : -(((-x_lo) + a - 1) / a) * a;
+                // the box's first element, x = iu0 + OFF in the staged
+                // layout, on the TMA alignment
+                using L = BoxLayout<T, PAIRED>;
+                const int a = L::ALIGN, xo = x_lo + L::OFF;
+                iu0 = ((xo >= 0) ? (xo / a) * a : -(((-xo) + a - 1) / a) * a) - L::OFF;
                 iv0 = y_lo;
-                const bool fits = (x_hi - iu0 + 1 <= BOX_W) && (y_hi - iv0 + 1 <= BOX_H);
+                // elements up to x_hi (the unpaired box's taps) or x_hi - 1
+                // (the paired element x_hi - 1 holds tap x_hi)
+                const bool fits = (x_hi - L::OFF - iu0 + 1 <= L::W) && (y_hi - iv0 + 1 <= BOX_H);
                 const bool clear_of_quirk = (x_hi <= W - 1) && (y_hi <= H - 1);
                 if (fits && clear_of_quirk) mode = MODE_SMEM;
             }
@@ -179,8 +236,8 @@ __device__ __forceinline__ void pass_meta(ViewMeta *meta, const ConeBpView *__re
     }
 }
 
-template <typename T, typename Tout>
-__global__ void __launch_bounds__(TB_X *TB_Y)
+template <typename T, typename Tout, bool PAIRED>
+__global__ void __launch_bounds__(TB_X *TB_Y, PYRONN_BP_MIN_BLOCKS(PAIRED))
     cone_bp_tma_kernel(const __grid_constant__ CUtensorMap tmap, const T *__restrict__ sino, Tout *__restrict__ vol,
                        const ConeBpView *__restrict__ views, const float *__restrict__ mult, int X, int Y, int Z,
                        int W, int H, int n_proj, int geom_batch, unsigned *__restrict__ err,
@@ -190,7 +247,9 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
     // TMA destinations must be 128-byte aligned: round the base up (the
     // launch reserves 128 spare bytes); every tile is a multiple of 128 bytes
     unsigned char *tile_base = dyn_smem + ((128u - (smem_addr(dyn_smem) & 127u)) & 127u);
-    T(*tiles)[BP_K][BOX_ELEMS] = reinterpret_cast<T(*)[BP_K][BOX_ELEMS]>(tile_base);  // [2][BP_K][BOX_ELEMS]
+    using E = typename BoxLayout<T, PAIRED>::E;
+    constexpr int BW = BoxLayout<T, PAIRED>::W, BE = BW * BOX_H;
+    E(*tiles)[BP_K][BE] = reinterpret_cast<E(*)[BP_K][BE]>(tile_base);  // [2][BP_K][BE]
     __shared__ __align__(16) ViewMeta meta[2][BP_K];
     __shared__ __align__(8) uint64_t full[2];
     __shared__ int s_failed;  // first pass whose wait gave up, n_pass if none (kept out of registers)
@@ -207,7 +266,7 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
     const T *sino_b = sino + (size_t)b * n_proj * H * W;
     const unsigned total = (unsigned)n_proj * (unsigned)H * (unsigned)W;
     const int n_pass = (n_proj + BP_K - 1) / BP_K;
-    constexpr unsigned TILE_BYTES = BOX_ELEMS * sizeof(T);
+    constexpr unsigned TILE_BYTES = BE * sizeof(E);
 
     if (tid == 0) {
         mbar_init(&full[0], 1);
@@ -233,11 +292,12 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
         for (int k = 0; k < BP_K; ++k) {
             const int n = p * BP_K + k;
             if (n < n_proj && meta[s][k].mode == MODE_SMEM)
-                tma_load_3d(&tiles[s][k][0], &tmap, meta[s][k].iu0, meta[s][k].iv0, b * n_proj + n, &full[s]);
+                tma_load_3d(&tiles[s][k][0], &tmap, meta[s][k].iu0 + BoxLayout<T, PAIRED>::OFF, meta[s][k].iv0,
+                            b * n_proj + n, &full[s]);
         }
     };
     if (warp == 0) {
-        pass_meta<T>(meta[0], pv, 0, n_proj, i0, j0, k0, W, H);
+        pass_meta<T, PAIRED>(meta[0], pv, 0, n_proj, i0, j0, k0, W, H);
         __syncwarp();
     }
     __syncthreads();
@@ -247,14 +307,16 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
 #pragma unroll
     for (int z = 0; z < TB_Z; ++z) acc[z] = 0.0f;
     const float fi = (float)i, fj = (float)j, fk = (float)k0;
-    constexpr unsigned MAX_IDX = BOX_ELEMS - BOX_W - 2, MAX_IDX2 = BOX_ELEMS - 2 * BOX_W - 2;
+    // a lerp reads elements idx and idx + 1 (one paired element)
+    constexpr unsigned LAST = PAIRED ? 1 : 2;
+    constexpr unsigned MAX_IDX = BE - BW - LAST, MAX_IDX2 = BE - 2 * BW - LAST;
     static_assert(TB_Z % 2 == 0, "the column loop takes voxels in pairs");
 
     for (int p = 0; p < n_pass; ++p) {
         const int cur = p & 1, nxt = cur ^ 1;
         __syncthreads();  // pass p-1 is done with stage nxt
         if (warp == 0 && p + 1 < n_pass) {
-            pass_meta<T>(meta[nxt], pv, (p + 1) * BP_K, n_proj, i0, j0, k0, W, H);
+            pass_meta<T, PAIRED>(meta[nxt], pv, (p + 1) * BP_K, n_proj, i0, j0, k0, W, H);
             __syncwarp();
             if (tid == 0) issue(p + 1, nxt);
         }
@@ -272,13 +334,13 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
             const float vb = fmaf(r1.x, fi, fmaf(r1.y, fj, fmaf(r1.z, fk, r1.w)));
             const float wb = fmaf(r2.x, fi, fmaf(r2.y, fj, fmaf(r2.z, fk, r2.w)));
             if (mode == MODE_SMEM && m.zconst) {
-                const T *tile = &tiles[cur][k][0];
+                const E *tile = &tiles[cur][k][0];
                 // fmaf(0, z, x) == x: these are the general loop's values at every z
                 const float rw = fast_rcp(wb), rw2 = rw * rw;
                 const FloorFrac fu = floor_frac(ub * rw - m.u0);
                 const float tx = fu.f;
                 // row of floor(lv) from its FloorFrac bits: the bias folded into one offset
-                const unsigned col = (unsigned)fu.i - (unsigned)FLOOR_BIAS * (unsigned)BOX_W;
+                const unsigned col = (unsigned)fu.i - (unsigned)FLOOR_BIAS * (unsigned)BW;
                 const float lv0 = fmaf(vb, rw, -m.v0), dlv = r1.z * rw;  // local v at z = 0, its step
                 if (dlv >= 0.0f && dlv < 0.999f) {
                     // rows of voxels z and z + 1 differ by 0 or 1: the pair
@@ -289,10 +351,11 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
                     for (int z = 0; z < TB_Z; z += 2) {
                         const float la = fmaf((float)z, dlv, lv0), lb = fmaf((float)(z + 1), dlv, lv0);
                         const FloorFrac fa = floor_frac(la), fb = floor_frac(lb);
-                        unsigned idx = (unsigned)fa.bits * (unsigned)BOX_W + col;
+                        unsigned idx = (unsigned)fa.bits * (unsigned)BW + col;
                         idx = min(idx, MAX_IDX2);  // memory safety only: the margin keeps idx in range
-                        const float p0 = smem_ulerp(tile + idx, tx), p1 = smem_ulerp(tile + idx + BOX_W, tx);
-                        const float p2 = smem_ulerp(tile + idx + 2 * BOX_W, tx);
+                        const float p0 = box_ulerp<T, PAIRED>(tile + idx, tx);
+                        const float p1 = box_ulerp<T, PAIRED>(tile + idx + BW, tx);
+                        const float p2 = box_ulerp<T, PAIRED>(tile + idx + 2 * BW, tx);
                         acc[z] = fmaf(lerp_ref(p0, p1, fa.f), rw2, acc[z]);
                         const bool up = fb.bits != fa.bits;
                         acc[z + 1] = fmaf(lerp_ref(up ? p1 : p0, up ? p2 : p1, fb.f), rw2, acc[z + 1]);
@@ -302,15 +365,15 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
                     for (int z = 0; z < TB_Z; ++z) {
                         const float lv = fmaf((float)z, dlv, lv0);
                         const FloorFrac fv = floor_frac(lv);
-                        unsigned idx = (unsigned)fv.bits * (unsigned)BOX_W + col;
+                        unsigned idx = (unsigned)fv.bits * (unsigned)BW + col;
                         idx = min(idx, MAX_IDX);  // memory safety only: the margin keeps idx in range
-                        const float val =
-                            lerp_ref(smem_ulerp(tile + idx, tx), smem_ulerp(tile + idx + BOX_W, tx), fv.f);
+                        const float val = lerp_ref(box_ulerp<T, PAIRED>(tile + idx, tx),
+                                                   box_ulerp<T, PAIRED>(tile + idx + BW, tx), fv.f);
                         acc[z] = fmaf(val, rw2, acc[z]);
                     }
                 }
             } else if (mode == MODE_SMEM) {
-                const T *tile = &tiles[cur][k][0];
+                const E *tile = &tiles[cur][k][0];
                 const float u0 = m.u0, v0 = m.v0;
 #pragma unroll
                 for (int z = 0; z < TB_Z; ++z) {
@@ -321,9 +384,10 @@ __global__ void __launch_bounds__(TB_X *TB_Y)
                     const float lv = fmaf(r1.z, fz, vb) * rw - v0;
                     const FloorFrac fu = floor_frac(lu), fv = floor_frac(lv);
                     const float tx = fu.f, ty = fv.f;
-                    unsigned idx = (unsigned)(fv.i * BOX_W + fu.i);
+                    unsigned idx = (unsigned)(fv.i * BW + fu.i);
                     idx = min(idx, MAX_IDX);  // memory safety only: the margin keeps idx in range
-                    const float val = lerp_ref(smem_ulerp(tile + idx, tx), smem_ulerp(tile + idx + BOX_W, tx), ty);
+                    const float val = lerp_ref(box_ulerp<T, PAIRED>(tile + idx, tx),
+                                               box_ulerp<T, PAIRED>(tile + idx + BW, tx), ty);
                     acc[z] = fmaf(val * rw, rw, acc[z]);
                 }
             } else {
@@ -395,35 +459,85 @@ CUtensorMapDataType tma_type<__half>()
     return CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
 }
 
-template <typename Tin, typename Tout>
-cudaError_t launch_typed(const void *sinogram, void *volume, const Dims3D &d, const ConeBpView *views,
-                         const float *mult, unsigned *err, int starve_last_pass, cudaStream_t stream)
+// The paired copy of a 16-bit sinogram: per detector row, element x holds
+// taps x - 1 (low half) and x (high half), x in [0, Wp), Wp = W + 1 rounded
+// up to 4 (16-byte rows), taps outside [0, W) zero.  Grid: x chunks of 256
+// elements by rows (a row per blockIdx.y, strided).
+template <typename T>
+__global__ void __launch_bounds__(256)
+    pair_sinogram_kernel(const T *__restrict__ sino, unsigned *__restrict__ paired, int W, int Wp, long long rows)
+{
+    const int x = blockIdx.x * 256 + threadIdx.x;
+    if (x >= Wp) return;
+    for (long long r = blockIdx.y; r < rows; r += gridDim.y) {
+        const unsigned short *row = reinterpret_cast<const unsigned short *>(sino + r * W);
+        const unsigned lo = (x >= 1 && x <= W) ? __ldg(row + x - 1) : 0u;
+        const unsigned hi = (x < W) ? __ldg(row + x) : 0u;
+        paired[r * Wp + x] = lo | (hi << 16);
+    }
+}
+
+inline int paired_row(int W)
+{
+    return (W + 1 + 3) / 4 * 4;
+}
+
+template <typename Tin, typename Tout, bool PAIRED>
+cudaError_t launch_kernel(const void *sinogram, const void *staged, void *volume, const Dims3D &d,
+                          const ConeBpView *views, const float *mult, unsigned *err, int starve_last_pass,
+                          cudaStream_t stream)
 {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return cudaErrorNotSupported;
+    using L = BoxLayout<Tin, PAIRED>;
+    using E = typename L::E;
+    const cuuint64_t row = PAIRED ? (cuuint64_t)paired_row(d.det_w) : (cuuint64_t)d.det_w;
     CUtensorMap map;
-    const cuuint64_t dims[3] = {(cuuint64_t)d.det_w, (cuuint64_t)d.det_h, (cuuint64_t)d.n_proj * d.batch};
-    const cuuint64_t strides[2] = {(cuuint64_t)d.det_w * sizeof(Tin), (cuuint64_t)d.det_w * d.det_h * sizeof(Tin)};
-    const cuuint32_t box[3] = {BOX_W, BOX_H, 1};
+    const cuuint64_t dims[3] = {row, (cuuint64_t)d.det_h, (cuuint64_t)d.n_proj * d.batch};
+    const cuuint64_t strides[2] = {row * sizeof(E), row * d.det_h * sizeof(E)};
+    const cuuint32_t box[3] = {(cuuint32_t)L::W, BOX_H, 1};
     const cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = enc(&map, tma_type<Tin>(), 3, const_cast<void *>(sinogram), dims, strides, box, estr,
+    const CUtensorMapDataType type = PAIRED ? CU_TENSOR_MAP_DATA_TYPE_UINT32 : tma_type<Tin>();
+    CUresult r = enc(&map, type, 3, const_cast<void *>(staged), dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
     const int zblocks = (d.vol_z + TB_Z - 1) / TB_Z;
     const dim3 block(TB_X, TB_Y, 1);
     const dim3 grid((d.vol_x + TB_X - 1) / TB_X, (d.vol_y + TB_Y - 1) / TB_Y, zblocks * d.batch);
-    static_assert((BOX_ELEMS * sizeof(float)) % 128 == 0 && (BOX_ELEMS * 2) % 128 == 0, "tile alignment");
-    const size_t smem = 2 * BP_K * BOX_ELEMS * sizeof(Tin) + 128;
+    static_assert((BOX_ELEMS * sizeof(float)) % 128 == 0 && (BOX_ELEMS * 2) % 128 == 0 &&
+                      (BOX_WP * BOX_H * 4) % 128 == 0,
+                  "tile alignment");
+    const size_t smem = 2 * BP_K * (size_t)L::W * BOX_H * sizeof(E) + 128;
     // set on every launch: the attribute belongs to the current device's copy
     // of the kernel, and the call is a cheap host-side update
-    cudaError_t e = cudaFuncSetAttribute(cone_bp_tma_kernel<Tin, Tout>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(cone_bp_tma_kernel<Tin, Tout, PAIRED>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    cone_bp_tma_kernel<Tin, Tout><<<grid, block, smem, stream>>>(map, (const Tin *)sinogram, (Tout *)volume, views, mult,
-                                                               d.vol_x, d.vol_y, d.vol_z, d.det_w, d.det_h, d.n_proj,
-                                                               d.geom_batch, err, starve_last_pass);
+    cone_bp_tma_kernel<Tin, Tout, PAIRED><<<grid, block, smem, stream>>>(
+        map, (const Tin *)sinogram, (Tout *)volume, views, mult, d.vol_x, d.vol_y, d.vol_z, d.det_w, d.det_h, d.n_proj,
+        d.geom_batch, err, starve_last_pass);
     return cudaGetLastError();
+}
+
+template <typename Tin, typename Tout>
+cudaError_t launch_typed(const void *sinogram, void *volume, const Dims3D &d, const ConeBpView *views,
+                         const float *mult, unsigned *err, int starve_last_pass, void *paired, cudaStream_t stream)
+{
+    if constexpr (sizeof(Tin) == 2) {
+        if (paired) {
+            const int Wp = paired_row(d.det_w);
+            const long long rows = (long long)d.batch * d.n_proj * d.det_h;
+            const dim3 pgrid((unsigned)((Wp + 255) / 256), (unsigned)(rows < 65535 ? rows : 65535));
+            pair_sinogram_kernel<Tin><<<pgrid, 256, 0, stream>>>((const Tin *)sinogram, (unsigned *)paired, d.det_w,
+                                                                 Wp, rows);
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+            return launch_kernel<Tin, Tout, true>(sinogram, paired, volume, d, views, mult, err, starve_last_pass,
+                                                  stream);
+        }
+    }
+    return launch_kernel<Tin, Tout, false>(sinogram, sinogram, volume, d, views, mult, err, starve_last_pass, stream);
 }
 
 }  // namespace
@@ -450,14 +564,21 @@ void cone_bp_tma_starve_last_pass(int enable)
     g_starve_last_pass.store(enable ? 1 : 0);
 }
 
+size_t cone_bp_tma_paired_bytes(int in_dtype, const Dims3D &d)
+{
+    if (dtype_size(in_dtype) != 2) return 0;
+    return (size_t)d.batch * d.n_proj * d.det_h * (size_t)paired_row(d.det_w) * sizeof(unsigned);
+}
+
 cudaError_t launch_cone_bp_tma(const void *sinogram, void *volume, int in_dtype, int out_dtype, const Dims3D &d,
-                               const ConeBpView *views, const float *mult, unsigned *err, cudaStream_t stream)
+                               const ConeBpView *views, const float *mult, unsigned *err, void *paired,
+                               cudaStream_t stream)
 {
     const int starve = g_starve_last_pass.load();
     return dispatch_dtypes(in_dtype, out_dtype, [&](auto tin, auto tout) {
         using Tin = typename decltype(tin)::type;
         using Tout = typename decltype(tout)::type;
-        return launch_typed<Tin, Tout>(sinogram, volume, d, views, mult, err, starve, stream);
+        return launch_typed<Tin, Tout>(sinogram, volume, d, views, mult, err, starve, paired, stream);
     });
 }
 

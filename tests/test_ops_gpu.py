@@ -230,6 +230,40 @@ def test_cone_backprojection_kernel_paths(cuda, dtype, case):
     assert rel_l2(out.cpu().numpy(), ref) < 1e-5
 
 
+@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])
+@pytest.mark.parametrize("tilted", [False, True])
+def test_cone_backprojection_paired_copy_is_bit_exact(cuda, dtype, tilted):
+    """Given the queried workspace, a 16-bit backprojection stages a paired
+    copy of the sinogram (tap u and u + 1 in one 32-bit element); given only
+    the views' part, it stages the sinogram itself.  The lerps are the same
+    operations on the same taps: the same bits, for the column loop of
+    circular views and the general loop of tilted ones."""
+    geo = _cone_geo(n_proj=12)
+    P = np.asarray(geo.projection_matrices).copy()
+    if tilted:
+        P[::2] = P[::2][:, :, [0, 2, 1, 3]]  # every other view rotates about y
+    args = (geo.volume_origin, geo.volume_spacing, P, geo.step_size, geo.projection_multiplier)
+    rng = np.random.Generator(np.random.PCG64(21))
+    sino = t(rng.uniform(0, 1, (2,) + geo.detector_shape), cuda, dtype)
+    gc = pl.ops.GeometryCone(2, cuda, *args, geo.detector_shape[0])
+    code = pl.ops.storage_code(dtype)
+    full = _capi.workspace_size("pyronn_cone_backprojection3d", 2, *geo.detector_shape, *geo.volume_shape, code, 0,
+                                gc.g)
+    views_only = 256 + (gc.g * geo.detector_shape[0] * 48 + 255) // 256 * 256
+    assert full > views_only
+    outs = []
+    for ws_bytes in (full, views_only):
+        ws = torch.empty(ws_bytes, dtype=torch.uint8, device=cuda)
+        out = torch.empty((2,) + geo.volume_shape, device=cuda)
+        _capi.call("pyronn_cone_backprojection3d", sino.data_ptr(), out.data_ptr(), code, 0, 0, 2,
+                   *geo.detector_shape, *geo.volume_shape, *gc.pointers(), gc.g, ws.data_ptr(), ws_bytes,
+                   torch.cuda.current_stream().cuda_stream)
+        outs.append(out.cpu())
+    assert torch.equal(outs[0], outs[1])
+    ref = oracle.cone_backprojection3d(rounded(sino), geo.volume_shape, *args)
+    assert rel_l2(outs[0].numpy(), ref) < 1e-5
+
+
 def test_workspace_error_flag_clear(cuda):
     geo = _cone_geo()
     p = torch.rand((1,) + geo.detector_shape, device=cuda)
