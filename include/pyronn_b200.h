@@ -202,8 +202,9 @@ PYRONN_API int pyronn_cone_projection3d(const void *volume, void *sinogram, int 
  * ------------------------------------------------------------------------- */
 /* Workspace bytes for a pyronn_cone_backprojection3d call with these
  * arguments: the per-view geometry and, for a 16-bit sinogram on the software
- * path, a paired copy of the sinogram (tap u and tap u + 1 in one 32-bit
- * element; one shared-memory load per lerp, the same results).  A workspace
+ * path with at least 100 voxels per detector pixel, a paired copy of the
+ * sinogram (tap u and tap u + 1 in one 32-bit element; one shared-memory load
+ * per lerp, the same results).  A workspace
  * of the per-view part alone -- this size with batch = 0 -- is accepted: the
  * call then stages the sinogram itself. */
 PYRONN_API size_t pyronn_cone_backprojection3d_workspace_size(int batch, int n_proj, int det_h, int det_w, int vol_z,

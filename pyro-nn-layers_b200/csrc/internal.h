@@ -91,8 +91,9 @@ cudaError_t launch_cone_scatter(const void *sinogram, float *volume, int in_dtyp
 
 // TMA-staged software backprojector (cone_bp_tma.cu); err = device error flag
 bool cone_bp_tma_supported(const void *sinogram, int in_dtype, const Dims3D &d);
-// Bytes of the paired copy of a 16-bit sinogram (0 for FP32): with it the
-// TMA backprojector stages 32-bit tap pairs, one shared-memory load per lerp.
+// Bytes of the paired copy of a 16-bit sinogram (0 for FP32, or where the
+// copy does not pay): with it the TMA backprojector stages 32-bit tap pairs,
+// one shared-memory load per lerp.
 size_t cone_bp_tma_paired_bytes(int in_dtype, const Dims3D &d);
 // `paired` (device, 16-byte aligned, cone_bp_tma_paired_bytes) or null.
 cudaError_t launch_cone_bp_tma(const void *sinogram, void *volume, int in_dtype, int out_dtype, const Dims3D &d,

@@ -237,8 +237,10 @@ def test_cone_backprojection_paired_copy_is_bit_exact(cuda, dtype, tilted):
     copy of the sinogram (tap u and u + 1 in one 32-bit element); given only
     the views' part, it stages the sinogram itself.  The lerps are the same
     operations on the same taps: the same bits, for the column loop of
-    circular views and the general loop of tilted ones."""
-    geo = _cone_geo(n_proj=12)
+    circular views and the general loop of tilted ones.  (The copy is made
+    where a detector pixel serves at least 100 voxel updates per view.)"""
+    geo = geometry.ConeBeam3D((64, 64, 64), (1.0, 1.0, 1.0), (40, 48), (2.4, 2.4), 12, 160.0, 260.0,
+                              projection_multiplier=0.8)
     P = np.asarray(geo.projection_matrices).copy()
     if tilted:
         P[::2] = P[::2][:, :, [0, 2, 1, 3]]  # every other view rotates about y
