@@ -337,10 +337,14 @@ __global__ void __launch_bounds__(TB_X *TB_Y, PYRONN_BP_MIN_BLOCKS(PAIRED))
                 const E *tile = &tiles[cur][k][0];
                 // fmaf(0, z, x) == x: these are the general loop's values at every z
                 const float rw = fast_rcp(wb), rw2 = rw * rw;
-                const FloorFrac fu = floor_frac(ub * rw - m.u0);
+                // floor and weight of u itself, the box origin subtracted
+                // from the integer floor: the tap and weight do not depend on
+                // where the box starts (paired and unpaired boxes align
+                // differently, and u - u0 in floating point rounds when u0 < 0)
+                const FloorFrac fu = floor_frac(__fmul_rn(ub, rw));
                 const float tx = fu.f;
                 // row of floor(lv) from its FloorFrac bits: the bias folded into one offset
-                const unsigned col = (unsigned)fu.i - (unsigned)FLOOR_BIAS * (unsigned)BW;
+                const unsigned col = (unsigned)(fu.i - m.iu0) - (unsigned)FLOOR_BIAS * (unsigned)BW;
                 const float lv0 = fmaf(vb, rw, -m.v0), dlv = r1.z * rw;  // local v at z = 0, its step
                 if (dlv >= 0.0f && dlv < 0.999f) {
                     // rows of voxels z and z + 1 differ by 0 or 1: the pair
@@ -374,17 +378,18 @@ __global__ void __launch_bounds__(TB_X *TB_Y, PYRONN_BP_MIN_BLOCKS(PAIRED))
                 }
             } else if (mode == MODE_SMEM) {
                 const E *tile = &tiles[cur][k][0];
-                const float u0 = m.u0, v0 = m.v0;
+                const int iu0 = m.iu0, iv0 = m.iv0;
 #pragma unroll
                 for (int z = 0; z < TB_Z; ++z) {
                     const float fz = (float)z;
                     const float rw = fast_rcp(fmaf(r2.z, fz, wb));
-                    // local box coordinates; the subtraction of an integer is exact
-                    const float lu = fmaf(r0.z, fz, ub) * rw - u0;
-                    const float lv = fmaf(r1.z, fz, vb) * rw - v0;
-                    const FloorFrac fu = floor_frac(lu), fv = floor_frac(lv);
+                    // floors and weights of (u, v) themselves, the box origin
+                    // subtracted from the integer floors (see the column loop)
+                    const float uu = __fmul_rn(fmaf(r0.z, fz, ub), rw);
+                    const float vv = __fmul_rn(fmaf(r1.z, fz, vb), rw);
+                    const FloorFrac fu = floor_frac(uu), fv = floor_frac(vv);
                     const float tx = fu.f, ty = fv.f;
-                    unsigned idx = (unsigned)(fv.i * BW + fu.i);
+                    unsigned idx = (unsigned)((fv.i - iv0) * BW + (fu.i - iu0));
                     idx = min(idx, MAX_IDX);  // memory safety only: the margin keeps idx in range
                     const float val = lerp_ref(box_ulerp<T, PAIRED>(tile + idx, tx),
                                                box_ulerp<T, PAIRED>(tile + idx + BW, tx), ty);
