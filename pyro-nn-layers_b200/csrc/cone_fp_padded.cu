@@ -389,9 +389,12 @@ __device__ __forceinline__ float march_cells(const ConeRay &ray, float step, boo
     const int Yc = Y + 2, Zc = Z + 2;
     const CellSampler<T, PACKED> s(cells + (Yc + 1) * Zc + 1, Zc, Yc * Zc);
     const int n = inside ? exact_sample_count(ray, step) : -1;
-    // eight samples per iteration for 16-bit cells, four for the 32-byte
-    // FP32 cells (whose loads need twice the registers)
-    return n > 0    ? march_counted<sizeof(T) == 4 ? 4 : 8>(ray, n, step, s)
+    // samples per iteration: four for the 32-byte FP32 cells (whose loads
+    // need twice the registers), six for FP16 and eight for BF16 cells
+    // (measured on the 512^3 forward: FP16 5 / 6 / 7 / 8 per iteration 84.3 /
+    // 80.3 / 82.4 / 81.7 ms; BF16 6 / 8: 85.2 / 84.4 ms)
+    constexpr int U = sizeof(T) == 4 ? 4 : (std::is_same<T, __half>::value ? 6 : 8);
+    return n > 0    ? march_counted<U>(ray, n, step, s)
            : inside ? march_x2(ray, step, s)
                     : march_x2(ray, step, ClampedCellSampler<T, PACKED>{s, xmax, ymax, zmax});
 }
