@@ -495,6 +495,22 @@ def test_cone_projection_non_circular_views(cuda, dtype):
     assert rel_l2(out.cpu().numpy(), ref) < CONE_FWD_TOL[dtype]
 
 
+@pytest.mark.parametrize("hw", [False, True])
+def test_cone_projection_volume_partly_off_detector(cuda, hw):
+    """Rays outside a view's detector footprint of the volume box skip their
+    set-up; with the volume shifted so that it projects partly off the
+    detector (and wholly off it in some views), the result still matches the
+    oracle, zeros included."""
+    geo = _cone_geo(n_proj=16)
+    origin = np.asarray(geo.volume_origin, np.float32) + np.array([6.0, 14.0, -11.0], np.float32)
+    args = (origin, geo.volume_spacing, geo.projection_matrices, geo.step_size, geo.projection_multiplier)
+    vol = phantoms.ellipsoid_phantom_3d(geo.volume_shape, geo.volume_spacing, seed=8, n=6)[0][None]
+    out = pl.cone_projection3d(t(vol, cuda), geo.detector_shape, *args, hardware_interp=hw)
+    ref = oracle.cone_projection3d(vol, geo.detector_shape, *args, hardware_interp=hw)
+    assert (ref == 0).any() and (ref != 0).any()
+    assert rel_l2(out.cpu().numpy(), ref) < (5e-4 if hw else 2e-5)
+
+
 def test_cone_projection_wide_fp16_range(cuda):
     """FP16 inputs whose magnitudes could overflow FP16 in the packed lerps'
     differences (above 32752) take FP32 y and x lerps: the cell copy flags
