@@ -30,11 +30,14 @@ mirrors ``REGISTER_OP("ConeProjection3D")`` (cc/ops/cone_projector_3D_OPKernel.c
 """
 from __future__ import annotations
 
+import collections
 import ctypes
+import hashlib
 import math
 import os
 from typing import Sequence
 
+import numpy as np
 import torch
 
 from . import _capi
@@ -61,8 +64,39 @@ def _shape(shape, n: int, what: str) -> list:
     return vals
 
 
+# Device copies of host geometry (numpy arrays, sequences, CPU tensors), by
+# content: a copy from pageable host memory waits for the stream's queued
+# work, so a loop that passes the same host geometry to every call would
+# otherwise serialise host and device at each call.  Bounded, least recently
+# used first out; keyed by the bytes, so a changed array is a new entry.
+_HOST_GEOM_CACHE: "collections.OrderedDict" = collections.OrderedDict()
+_HOST_GEOM_CACHE_SIZE = 64
+
+
+def _host_geometry_on_device(t, device) -> torch.Tensor:
+    a = np.ascontiguousarray(t.numpy() if isinstance(t, torch.Tensor) else np.asarray(t), dtype=np.float32)
+    dev = torch.device(device)
+    if dev.type == "cuda" and dev.index is None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+    key = (str(dev), a.shape, hashlib.blake2b(a.tobytes(), digest_size=16).digest())
+    hit = _HOST_GEOM_CACHE.get(key)
+    if hit is not None:
+        _HOST_GEOM_CACHE.move_to_end(key)
+        return hit
+    d = torch.from_numpy(a.copy()).to(dev)
+    if dev.type == "cuda":
+        # the copy is complete before any stream uses the cached tensor
+        torch.cuda.current_stream(dev).synchronize()
+    _HOST_GEOM_CACHE[key] = d
+    while len(_HOST_GEOM_CACHE) > _HOST_GEOM_CACHE_SIZE:
+        _HOST_GEOM_CACHE.popitem(last=False)
+    return d
+
+
 def _geom(t, batch: int, row_shape: Sequence[int], device, what: str):
     """Returns (contiguous float32 tensor [g, *row_shape] on device, g)."""
+    if not (isinstance(t, torch.Tensor) and t.device.type == "cuda"):
+        t = _host_geometry_on_device(t.detach() if isinstance(t, torch.Tensor) else t, device)
     t = torch.as_tensor(t, dtype=torch.float32)
     row_numel = 1
     for s in row_shape:

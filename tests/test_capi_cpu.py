@@ -135,3 +135,21 @@ def test_trajectory_builders_reject_bad_arguments():
     g = lib.pyronn_circular_ray_vectors_2d
     assert g(FAKE, -1, 3.14, 0.0, None) == _capi.ERROR_INVALID_ARGUMENT
     assert g(FAKE, 4, float("inf"), 0.0, None) == _capi.ERROR_INVALID_ARGUMENT
+
+
+def test_host_geometry_cache_is_keyed_by_content():
+    """Host geometry passed to the ops is copied to the device once per
+    content (a copy from pageable memory would wait for the stream's queued
+    work on every call); a changed array is a new entry, the cache is bounded."""
+    np = pytest.importorskip("numpy")
+    pytest.importorskip("torch")
+    from pyronn_layers import ops
+    a = np.arange(12, dtype=np.float32)
+    d1 = ops._host_geometry_on_device(a, "cpu")
+    assert ops._host_geometry_on_device(a.copy(), "cpu") is d1
+    a[0] = 5.0
+    d3 = ops._host_geometry_on_device(a, "cpu")
+    assert d3 is not d1 and float(d3[0]) == 5.0 and float(d1[0]) == 0.0
+    for k in range(ops._HOST_GEOM_CACHE_SIZE + 8):
+        ops._host_geometry_on_device(np.full(3, float(k), np.float32), "cpu")
+    assert len(ops._HOST_GEOM_CACHE) <= ops._HOST_GEOM_CACHE_SIZE
