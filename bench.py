@@ -61,20 +61,20 @@ PHANTOM_ELLIPSOIDS = 32
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
 # the dominant kernel, from a one-pass ncu capture of one forward launch of
 #   python bench.py --steps 1 --warmup 3 --no-cpu-baseline
-# (profiles/dram_cone512.md), keyed by (workload, volume storage, sinogram
-# storage, hardware_interp)
+# keyed by (workload, volume storage, sinogram storage, hardware_interp)
 NCU_DRAM_BYTES = {
     ("cone512", "fp16", "fp16", False): 38.485e9 + 0.573e9,
 }
-# ncu counters of the forward kernel (profiles/cone_fp_padded_kernel_cone256_fp16.md,
-# a --set full capture at 256^3): issue activity, and L2 -> SM bytes per ray
-# sample scaled to a 512^3 launch by its sample count
+# ncu counters of the forward kernel from a section capture of its first
+# launch at 256^3 (issue activity, lanes, instructions per ray sample; L2 ->
+# SM bytes per ray sample from a --set full capture at 256^3, scaling with the
+# sample count)
 NCU_FORWARD_COUNTERS = {
     ("cone512", "fp16", "fp16", False): {
-        "issue_active": 0.829, "lanes_active_per_warp_instruction": 26.97,
-        "thread_instructions_per_sample": 44.7, "lts2xbar_bytes_per_sample_256": 11.0,
+        "issue_active": 0.805, "lanes_active_per_warp_instruction": 26.71,
+        "thread_instructions_per_sample": 36.2, "lts2xbar_bytes_per_sample_256": 11.0,
         "source": "profiles/cone_fp_padded_kernel_cone256_fp16.md (256^3 capture; L2 -> SM bytes per sample "
-                  "from the earlier full capture, scaling with the samples)"},
+                  "from the full capture, scaling with the samples)"},
 }
 # kernels of ours launched per fwd+back step (geometry preparation, view
 # classification, the two volume copies, forward; preparation, backprojection)
@@ -739,7 +739,10 @@ def run_ours(args, cfg):
                 "overlap": "two slots: the H2D copy of step i+1 and the D2H copy of step i run on their own "
                            "streams during step i's projections; every step's input and result cross the host "
                            "link inside the timed region"},
-        "gpu_launches": LAUNCHES_PER_STEP[hw] * args.steps,
+        # (+1 per step where the backprojection pairs a 16-bit sinogram: at
+        # least 100 voxels per detector pixel)
+        "gpu_launches": (LAUNCHES_PER_STEP[hw] + int(not hw and sino_storage != torch.float32
+                                                    and Z * Y * X >= 100 * H * W)) * args.steps,
         "clocks": clocks,
     }
 
