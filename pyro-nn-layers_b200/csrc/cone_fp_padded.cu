@@ -218,21 +218,26 @@ struct Wide16<__nv_bfloat16> {
 // z-fastest cell copy: element [xc][yc][zc], xc in [0, X+1], yc in [0, Y+1],
 // zc in [0, Z+1], holds the cell whose low corner is voxel (xc-1, yc-1, zc-1)
 // (V zero outside the volume), i.e. the taps of every floor in [-1, N].
-// A block reads a 33 (x) x 33 (z) x 2 (y) tile along x and writes 32 (z) x
-// 32 (x) cells along z.  Skipped when no view is in z mode.
+// A block reads a 33 (x) x 33 (z) x (CELL_PLANES + 1) (y) tile along x --
+// each plane once for its CELL_PLANES cell planes -- and writes 32 (z) x 32
+// (x) x CELL_PLANES cells along z (measured at 512^3, one / four / eight
+// planes per block: 1.07 / 0.88 / 0.84 ms).  Skipped when no view is in z
+// mode.
+constexpr int CELL_PLANES = 8;
 template <typename T>
 __global__ void __launch_bounds__(PAD_TILE *8) pad_cells_kernel(const T *__restrict__ src,
                                                                  typename Cell<T>::type *__restrict__ dst, int X,
                                                                  int Y, int Z, unsigned *__restrict__ flags)
 {
     if (!flags[FLAG_NEED_Z]) return;
-    __shared__ T tile[2][PAD_TILE + 1][PAD_TILE + 2];  // [y - (yc-1)][z - (zc0-1)][x - (xc0-1)]
+    // [y - (yc0-1)][z - (zc0-1)][x - (xc0-1)]
+    __shared__ T tile[CELL_PLANES + 1][PAD_TILE + 1][PAD_TILE + 2];
     bool wide = false;
     const int Yc = Y + 2, Zc = Z + 2;
-    const int xc0 = blockIdx.x * PAD_TILE, yc = blockIdx.y, zc0 = blockIdx.z * PAD_TILE;
-    for (int rr = threadIdx.y; rr < 2 * (PAD_TILE + 1); rr += 8) {
+    const int xc0 = blockIdx.x * PAD_TILE, yc0 = blockIdx.y * CELL_PLANES, zc0 = blockIdx.z * PAD_TILE;
+    for (int rr = threadIdx.y; rr < (CELL_PLANES + 1) * (PAD_TILE + 1); rr += 8) {
         const int dy = rr / (PAD_TILE + 1), r = rr % (PAD_TILE + 1);
-        const int y = yc - 1 + dy, z = zc0 - 1 + r;
+        const int y = yc0 - 1 + dy, z = zc0 - 1 + r;
         const bool yz_in = y >= 0 && y < Y && z >= 0 && z < Z;
         for (int c = threadIdx.x; c < PAD_TILE + 1; c += PAD_TILE) {
             const int x = xc0 - 1 + c;
@@ -245,12 +250,20 @@ __global__ void __launch_bounds__(PAD_TILE *8) pad_cells_kernel(const T *__restr
     if (__syncthreads_or(wide) && threadIdx.x == 0 && threadIdx.y == 0) atomicOr(&flags[FLAG_WIDE], 1u);
     const int tz = threadIdx.x, zc = zc0 + tz;
     if (zc >= Zc) return;
-    for (int c = threadIdx.y; c < PAD_TILE; c += 8) {
-        const int xc = xc0 + c;
-        if (xc >= X + 2) break;
-        const T v[8] = {tile[0][tz][c], tile[0][tz][c + 1], tile[0][tz + 1][c], tile[0][tz + 1][c + 1],
-                        tile[1][tz][c], tile[1][tz][c + 1], tile[1][tz + 1][c], tile[1][tz + 1][c + 1]};
-        dst[((size_t)xc * Yc + yc) * Zc + zc] = Cell<T>::make(v);
+#pragma unroll
+    for (int pl = 0; pl < CELL_PLANES; ++pl) {
+        const int yc = yc0 + pl;
+        if (yc >= Yc) break;
+#pragma unroll
+        for (int k = 0; k < PAD_TILE / 8; ++k) {
+            const int c = threadIdx.y + 8 * k, xc = xc0 + c;
+            if (xc < X + 2) {
+                const T v[8] = {tile[pl][tz][c],     tile[pl][tz][c + 1],     tile[pl][tz + 1][c],
+                                tile[pl][tz + 1][c + 1], tile[pl + 1][tz][c], tile[pl + 1][tz][c + 1],
+                                tile[pl + 1][tz + 1][c], tile[pl + 1][tz + 1][c + 1]};
+                dst[((size_t)xc * Yc + yc) * Zc + zc] = Cell<T>::make(v);
+            }
+        }
     }
 }
 
@@ -494,7 +507,8 @@ cudaError_t launch_typed(const void *volume, void *sinogram, const Dims3D &d, co
     const dim3 pblock(PAD_TILE, 8);
     const dim3 pgrid((unsigned)((Xp + PAD_TILE - 1) / PAD_TILE), (unsigned)((Yp + PAD_TILE - 1) / PAD_TILE),
                      (unsigned)Zp);
-    const dim3 cgrid((unsigned)((Xc + PAD_TILE - 1) / PAD_TILE), (unsigned)Yc, (unsigned)((Zc + PAD_TILE - 1) / PAD_TILE));
+    const dim3 cgrid((unsigned)((Xc + PAD_TILE - 1) / PAD_TILE), (unsigned)((Yc + CELL_PLANES - 1) / CELL_PLANES),
+                     (unsigned)((Zc + PAD_TILE - 1) / PAD_TILE));
     const dim3 block(PB_X, PB_Y);
     const unsigned grid = ray_block_count(d.det_w, d.det_h, d.n_proj);
     for (int b = 0; b < d.batch; ++b) {
