@@ -220,9 +220,9 @@ struct Wide16<__nv_bfloat16> {
 // (V zero outside the volume), i.e. the taps of every floor in [-1, N].
 // A block reads a 33 (x) x 33 (z) x (CELL_PLANES + 1) (y) tile along x --
 // each plane once for its CELL_PLANES cell planes -- and writes 32 (z) x 32
-// (x) x CELL_PLANES cells along z (measured at 512^3, one / four / eight
-// planes per block: 1.07 / 0.88 / 0.84 ms).  Skipped when no view is in z
-// mode.
+// (x) x CELL_PLANES cells along z (at 512^3 the copy took 1.07 ms with one
+// plane per block, 0.88 ms with four; the whole forward op 80.39 / 80.14 /
+// 80.10 ms with one / four / eight).  Skipped when no view is in z mode.
 constexpr int CELL_PLANES = 8;
 template <typename T>
 __global__ void __launch_bounds__(PAD_TILE *8) pad_cells_kernel(const T *__restrict__ src,
