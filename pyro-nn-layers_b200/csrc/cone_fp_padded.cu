@@ -21,6 +21,7 @@
 // does), so results match the direct path.
 #include <math_constants.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "common.cuh"
@@ -34,6 +35,7 @@ namespace {
 constexpr int PB_X = 32;
 constexpr int PB_Y = 8;
 constexpr int PAD_TILE = 32;
+constexpr size_t PAD_Z_BLOCKS = 16;  // z blocks of the xy-mode padded copy, each striding over planes
 // workspace header words (after the error flag) set by classify_views_kernel
 // (FLAG_WIDE: a 16-bit input holds magnitudes whose differences may not fit
 // the storage type, so the cells take the FP32 y and x lerps)
@@ -276,25 +278,30 @@ __global__ void __launch_bounds__(PAD_TILE *8) pad_volume_kernel(const T *__rest
 {
     if (!flags[FLAG_NEED_XY]) return;
     __shared__ T tile[PAD_TILE][PAD_TILE + 1];
-    const int Xp = X + 3, Yp = Y + 3;
-    const int zp = blockIdx.z;   // padded z
-    const int z = zp - 1;        // source z
+    const int Xp = X + 3, Yp = Y + 3, Zp = Z + 3;
     const int x0 = blockIdx.x * PAD_TILE - 1, y0 = blockIdx.y * PAD_TILE - 1;  // padded tile origin - 1
-    const bool zin = z >= 0 && z < Z;
-    // load a tile (source coordinates x0.., y0..) and write the x-fastest copy
-    for (int r = threadIdx.y; r < PAD_TILE; r += 8) {
-        const int y = y0 + r, x = x0 + threadIdx.x;
-        T v = T(0.0f);
-        if (zin && y >= 0 && y < Y && x >= 0 && x < X) v = src[((size_t)z * Y + y) * X + x];
-        tile[r][threadIdx.x] = v;
-        const int xp = x + 1, yp = y + 1;
-        if (xp < Xp && yp < Yp) xfast[((size_t)zp * Yp + yp) * Xp + xp] = v;
-    }
-    __syncthreads();
-    // transposed write of the y-fastest copy
-    for (int r = threadIdx.y; r < PAD_TILE; r += 8) {
-        const int xp = x0 + r + 1, yp = y0 + threadIdx.x + 1;
-        if (xp < Xp && yp < Yp) yfast[((size_t)zp * Xp + xp) * Yp + yp] = tile[threadIdx.x][r];
+    // padded z planes strided over the grid's z blocks: a small grid, so a
+    // call with no xy-mode view (every circular trajectory) costs one wave of
+    // blocks that return at once
+    for (int zp = blockIdx.z; zp < Zp; zp += gridDim.z) {
+        const int z = zp - 1;  // source z
+        const bool zin = z >= 0 && z < Z;
+        __syncthreads();  // the previous plane's transposed reads are done
+        // load a tile (source coordinates x0.., y0..) and write the x-fastest copy
+        for (int r = threadIdx.y; r < PAD_TILE; r += 8) {
+            const int y = y0 + r, x = x0 + threadIdx.x;
+            T v = T(0.0f);
+            if (zin && y >= 0 && y < Y && x >= 0 && x < X) v = src[((size_t)z * Y + y) * X + x];
+            tile[r][threadIdx.x] = v;
+            const int xp = x + 1, yp = y + 1;
+            if (xp < Xp && yp < Yp) xfast[((size_t)zp * Yp + yp) * Xp + xp] = v;
+        }
+        __syncthreads();
+        // transposed write of the y-fastest copy
+        for (int r = threadIdx.y; r < PAD_TILE; r += 8) {
+            const int xp = x0 + r + 1, yp = y0 + threadIdx.x + 1;
+            if (xp < Xp && yp < Yp) yfast[((size_t)zp * Xp + xp) * Yp + yp] = tile[threadIdx.x][r];
+        }
     }
 }
 
@@ -506,7 +513,7 @@ cudaError_t launch_typed(const void *volume, void *sinogram, const Dims3D &d, co
     classify_views_kernel<<<(nviews + 127) / 128, 128, 0, stream>>>(views, nviews, flags);
     const dim3 pblock(PAD_TILE, 8);
     const dim3 pgrid((unsigned)((Xp + PAD_TILE - 1) / PAD_TILE), (unsigned)((Yp + PAD_TILE - 1) / PAD_TILE),
-                     (unsigned)Zp);
+                     (unsigned)std::min<size_t>(Zp, PAD_Z_BLOCKS));
     const dim3 cgrid((unsigned)((Xc + PAD_TILE - 1) / PAD_TILE), (unsigned)((Yc + CELL_PLANES - 1) / CELL_PLANES),
                      (unsigned)((Zc + PAD_TILE - 1) / PAD_TILE));
     const dim3 block(PB_X, PB_Y);
