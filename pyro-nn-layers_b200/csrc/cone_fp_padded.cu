@@ -155,12 +155,13 @@ struct Cell16 {
     // 11 instructions for the seven lerps instead of 16.  Differences of the
     // interpolated pair must fit the storage type: used when every input
     // magnitude is below Wide16<T16>::limit (FLAG_WIDE clear).
-    __device__ static float trilinear_packed(const uint4 *c, float tz, float ty, float tx)
+    // (tz2 = 2 tz, the z weight in half-voxel units)
+    __device__ static float trilinear_packed(const uint4 *c, float tz2f, float ty, float tx)
     {
         const uint4 w = __ldg(c);
         unsigned tz2, ty2, zy0, zy1, dy, yv;
         if (BF16) {
-            asm("cvt.rn.bf16x2.f32 %0, %1, %1;" : "=r"(tz2) : "f"(tz + tz));
+            asm("cvt.rn.bf16x2.f32 %0, %1, %1;" : "=r"(tz2) : "f"(tz2f));
             asm("cvt.rn.bf16x2.f32 %0, %1, %1;" : "=r"(ty2) : "f"(ty));
             asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(zy0) : "r"(tz2), "r"(w.y), "r"(w.x));
             asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(zy1) : "r"(tz2), "r"(w.w), "r"(w.z));
@@ -169,7 +170,7 @@ struct Cell16 {
             const float lo = __uint_as_float(yv << 16);
             return fmaf(tx, sub_f32_bf16<true>(yv, lo), lo);
         } else {
-            asm("cvt.rn.f16x2.f32 %0, %1, %1;" : "=r"(tz2) : "f"(tz + tz));
+            asm("cvt.rn.f16x2.f32 %0, %1, %1;" : "=r"(tz2) : "f"(tz2f));
             asm("cvt.rn.f16x2.f32 %0, %1, %1;" : "=r"(ty2) : "f"(ty));
             asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(zy0) : "r"(tz2), "r"(w.y), "r"(w.x));
             asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(zy1) : "r"(tz2), "r"(w.w), "r"(w.z));
@@ -363,24 +364,42 @@ __device__ __forceinline__ bool march_inside(const ConeRay &r, int X, int Y, int
            fmaxf(y0, y1) <= Y + 0.5f && fmaxf(z0, z1) <= Z + 0.5f;
 }
 
+// floor and fraction of z2 / 2 from z2 = 2 z (exact: scaling by two commutes
+// with every rounding here): bits = floor(z) + FLOOR_BIAS_2Z, f = 2 (z - floor(z))
+constexpr int FLOOR_BIAS_2Z = 0x4BC00000;  // bit pattern of 1.5 * 2^24
+__device__ __forceinline__ FloorFrac floor_frac_2z(float z2)
+{
+    const float magic = 25165824.0f;  // 1.5 * 2^24: ulp 2, so the sum rounds down to an even integer
+    const float y = __fadd_rd(z2, magic);
+    FloorFrac r;
+    r.bits = __float_as_int(y);
+    r.i = r.bits - FLOOR_BIAS_2Z;
+    r.f = __fadd_rn(z2, -__fadd_rn(y, -magic));
+    return r;
+}
+
 // Trilinear interpolation from the cell copy: one cell load gives the eight
 // taps.  `origin` points at the cell of floor (0, 0, 0); the floor bias of
 // the three FloorFrac bit patterns is folded into one per-sampler offset.
+// The packed sampler takes z in half-voxel units (Z2): its floor then gives
+// the doubled z weight the half-difference lerp multiplies by, with no
+// doubling per sample.
 template <typename T, bool PACKED>
 struct CellSampler {
+    static constexpr bool Z2 = PACKED;
     const typename Cell<T>::type *origin;
     unsigned s_y, s_x;  // cell strides of y and x (z is fastest)
-    unsigned bias;      // -FLOOR_BIAS * (s_x + s_y + 1), modulo 2^32
+    unsigned bias;      // -(FLOOR_BIAS * (s_x + s_y) + the z floor's bias), modulo 2^32
 
     __device__ CellSampler(const typename Cell<T>::type *o, int sy, int sx)
         : origin(o), s_y((unsigned)sy), s_x((unsigned)sx),
-          bias(0u - (unsigned)FLOOR_BIAS * ((unsigned)sx + (unsigned)sy + 1u))
+          bias(0u - (unsigned)FLOOR_BIAS * ((unsigned)sx + (unsigned)sy) - (unsigned)(Z2 ? FLOOR_BIAS_2Z : FLOOR_BIAS))
     {
     }
 
     __device__ __forceinline__ float operator()(float x, float y, float z) const
     {
-        const FloorFrac fx = floor_frac(x), fy = floor_frac(y), fz = floor_frac(z);
+        const FloorFrac fx = floor_frac(x), fy = floor_frac(y), fz = Z2 ? floor_frac_2z(z) : floor_frac(z);
         const unsigned idx = (unsigned)fx.bits * s_x + (unsigned)fy.bits * s_y + (unsigned)fz.bits + bias;
         // the reference's order: lerp in z, then y, then x
         if constexpr (PACKED)
@@ -393,10 +412,10 @@ struct CellSampler {
 template <typename T, bool PACKED>
 struct ClampedCellSampler {
     CellSampler<T, PACKED> s;
-    float xmax, ymax, zmax;
+    float xmax, ymax, zlo, zmax;  // z bounds in the sampler's z units
     __device__ __forceinline__ float operator()(float x, float y, float z) const
     {
-        return s(fminf(fmaxf(x, -1.0f), xmax), fminf(fmaxf(y, -1.0f), ymax), fminf(fmaxf(z, -1.0f), zmax));
+        return s(fminf(fmaxf(x, -1.0f), xmax), fminf(fmaxf(y, -1.0f), ymax), fminf(fmaxf(z, zlo), zmax));
     }
 };
 
@@ -414,9 +433,14 @@ __device__ __forceinline__ float march_cells(const ConeRay &ray, float step, boo
     // (measured on the 512^3 forward: FP16 5 / 6 / 7 / 8 per iteration 84.3 /
     // 80.3 / 82.4 / 81.7 ms; BF16 6 / 8: 85.2 / 84.4 ms)
     constexpr int U = sizeof(T) == 4 ? 4 : (std::is_same<T, __half>::value ? 6 : 8);
-    return n > 0    ? march_counted<U>(ray, n, step, s)
-           : inside ? march_x2(ray, step, s)
-                    : march_x2(ray, step, ClampedCellSampler<T, PACKED>{s, xmax, ymax, zmax});
+    // the packed sampler's z in half-voxel units: the ray's z scaled by two
+    // (fmaf(a, 2 dz, 2 oz) = 2 fmaf(a, dz, oz) exactly), clamps with it
+    ConeRay r = ray;
+    float zlo = -1.0f;
+    if (CellSampler<T, PACKED>::Z2) r.dz *= 2.0f, r.oz *= 2.0f, zlo = -2.0f, zmax *= 2.0f;
+    return n > 0    ? march_counted<U>(r, n, step, s)
+           : inside ? march_x2(r, step, s)
+                    : march_x2(r, step, ClampedCellSampler<T, PACKED>{s, xmax, ymax, zlo, zmax});
 }
 
 // Grid: one dimension, ray_block_count blocks in ray_block order (four
