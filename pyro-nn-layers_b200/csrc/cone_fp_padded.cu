@@ -218,8 +218,9 @@ struct Wide16<__nv_bfloat16> {
     __device__ static bool exceeds(__nv_bfloat16 v) { return fabsf(__bfloat162float(v)) > 8.5e37f; }
 };
 
-// z-fastest cell copy: element [xc][yc][zc], xc in [0, X+1], yc in [0, Y+1],
-// zc in [0, Z+1], holds the cell whose low corner is voxel (xc-1, yc-1, zc-1)
+// z-fastest cell copy: element [xc][yc][zc], xc in [0, X+1] (pitch s_x >=
+// (Y+2) (Z+2), from cell_x_pitch), yc in [0, Y+1], zc in [0, Z+1], holds the
+// cell whose low corner is voxel (xc-1, yc-1, zc-1)
 // (V zero outside the volume), i.e. the taps of every floor in [-1, N].
 // A block reads a 33 (x) x 33 (z) x (CELL_PLANES + 1) (y) tile along x --
 // each plane once for its CELL_PLANES cell planes -- and writes 32 (z) x 32
@@ -230,7 +231,7 @@ constexpr int CELL_PLANES = 8;
 template <typename T>
 __global__ void __launch_bounds__(PAD_TILE *8) pad_cells_kernel(const T *__restrict__ src,
                                                                  typename Cell<T>::type *__restrict__ dst, int X,
-                                                                 int Y, int Z, unsigned *__restrict__ flags)
+                                                                 int Y, int Z, int s_x, unsigned *__restrict__ flags)
 {
     if (!flags[FLAG_NEED_Z]) return;
     // [y - (yc0-1)][z - (zc0-1)][x - (xc0-1)]
@@ -264,7 +265,7 @@ __global__ void __launch_bounds__(PAD_TILE *8) pad_cells_kernel(const T *__restr
                 const T v[8] = {tile[pl][tz][c],     tile[pl][tz][c + 1],     tile[pl][tz + 1][c],
                                 tile[pl][tz + 1][c + 1], tile[pl + 1][tz][c], tile[pl + 1][tz][c + 1],
                                 tile[pl + 1][tz + 1][c], tile[pl + 1][tz + 1][c + 1]};
-                dst[((size_t)xc * Yc + yc) * Zc + zc] = Cell<T>::make(v);
+                dst[(size_t)xc * s_x + (size_t)yc * Zc + zc] = Cell<T>::make(v);
             }
         }
     }
@@ -378,34 +379,44 @@ __device__ __forceinline__ FloorFrac floor_frac_2z(float z2)
     return r;
 }
 
+// The cell index with the three floor biases folded in, FLOOR_BIAS (s_x +
+// s_y) + z bias + index (mod 2^32), is the bias plus the index without
+// wrapping when the x pitch s_x is chosen for it (cell_x_pitch): then the
+// biased index addresses the copy through one unsigned 32 x 32 -> 64-bit
+// multiply-add from a base that takes the bias back out.
+__host__ __device__ inline unsigned cell_index_bias(unsigned s_x, unsigned s_y, bool z2)
+{
+    return (unsigned)FLOOR_BIAS * (s_x + s_y) + (unsigned)(z2 ? FLOOR_BIAS_2Z : FLOOR_BIAS);
+}
+
 // Trilinear interpolation from the cell copy: one cell load gives the eight
-// taps.  `origin` points at the cell of floor (0, 0, 0); the floor bias of
-// the three FloorFrac bit patterns is folded into one per-sampler offset.
-// The packed sampler takes z in half-voxel units (Z2): its floor then gives
-// the doubled z weight the half-difference lerp multiplies by, with no
+// taps.  The packed sampler takes z in half-voxel units (Z2): its floor then
+// gives the doubled z weight the half-difference lerp multiplies by, with no
 // doubling per sample.
 template <typename T, bool PACKED>
 struct CellSampler {
+    using C = typename Cell<T>::type;
     static constexpr bool Z2 = PACKED;
-    const typename Cell<T>::type *origin;
-    unsigned s_y, s_x;  // cell strides of y and x (z is fastest)
-    unsigned bias;      // -(FLOOR_BIAS * (s_x + s_y) + the z floor's bias), modulo 2^32
+    unsigned long long base;  // address of biased index 0 (modulo 2^64)
+    unsigned s_y, s_x;        // cell strides of y and x (z is fastest)
 
-    __device__ CellSampler(const typename Cell<T>::type *o, int sy, int sx)
-        : origin(o), s_y((unsigned)sy), s_x((unsigned)sx),
-          bias(0u - (unsigned)FLOOR_BIAS * ((unsigned)sx + (unsigned)sy) - (unsigned)(Z2 ? FLOOR_BIAS_2Z : FLOOR_BIAS))
+    // `cells` is the copy's first cell, whose floor is (-1, -1, -1)
+    __device__ CellSampler(const C *cells, int sy, int sx) : s_y((unsigned)sy), s_x((unsigned)sx)
     {
+        const unsigned long long origin = (unsigned long long)s_x + s_y + 1;  // index of floor (0, 0, 0)
+        base = (unsigned long long)cells + sizeof(C) * (origin - cell_index_bias(s_x, s_y, Z2));
     }
 
     __device__ __forceinline__ float operator()(float x, float y, float z) const
     {
         const FloorFrac fx = floor_frac(x), fy = floor_frac(y), fz = Z2 ? floor_frac_2z(z) : floor_frac(z);
-        const unsigned idx = (unsigned)fx.bits * s_x + (unsigned)fy.bits * s_y + (unsigned)fz.bits + bias;
+        const unsigned t = (unsigned)fx.bits * s_x + (unsigned)fy.bits * s_y + (unsigned)fz.bits;
+        const C *c = (const C *)(base + (unsigned long long)t * sizeof(C));
         // the reference's order: lerp in z, then y, then x
         if constexpr (PACKED)
-            return Cell<T>::trilinear_packed(origin + (int)idx, fz.f, fy.f, fx.f);
+            return Cell<T>::trilinear_packed(c, fz.f, fy.f, fx.f);
         else
-            return Cell<T>::trilinear(origin + (int)idx, fz.f, fy.f, fx.f);
+            return Cell<T>::trilinear(c, fz.f, fy.f, fx.f);
     }
 };
 
@@ -422,17 +433,18 @@ struct ClampedCellSampler {
 // The march of one z-mode ray over the cell copy.
 template <typename T, bool PACKED>
 __device__ __forceinline__ float march_cells(const ConeRay &ray, float step, bool inside,
-                                             const typename Cell<T>::type *cells, int Y, int Z, float xmax,
+                                             const typename Cell<T>::type *cells, int Z, int s_x, float xmax,
                                              float ymax, float zmax)
 {
-    const int Yc = Y + 2, Zc = Z + 2;
-    const CellSampler<T, PACKED> s(cells + (Yc + 1) * Zc + 1, Zc, Yc * Zc);
+    const CellSampler<T, PACKED> s(cells, Z + 2, s_x);
     const int n = inside ? exact_sample_count(ray, step) : -1;
     // samples per iteration: four for the 32-byte FP32 cells (whose loads
-    // need twice the registers), six for FP16 and eight for BF16 cells
-    // (measured on the 512^3 forward: FP16 5 / 6 / 7 / 8 per iteration 84.3 /
-    // 80.3 / 82.4 / 81.7 ms; BF16 6 / 8: 85.2 / 84.4 ms)
-    constexpr int U = sizeof(T) == 4 ? 4 : (std::is_same<T, __half>::value ? 6 : 8);
+    // need twice the registers), seven for FP16 and six for BF16 cells
+    // (measured on the 512^3 forward, the best of a sweep whose times follow
+    // the compiler's schedule more than the count: FP16 4 / 5 / 6 / 7 / 8 per
+    // iteration 82.3 / 80.3 / 79.0 / 77.2 / 77.4 ms; BF16 5 / 6 / 7 / 8 / 10:
+    // 76.0 / 74.5 / 77.5 / 76.0 / 75.8 ms)
+    constexpr int U = sizeof(T) == 4 ? 4 : (std::is_same<T, __half>::value ? 7 : 6);
     // the packed sampler's z in half-voxel units: the ray's z scaled by two
     // (fmaf(a, 2 dz, 2 oz) = 2 fmaf(a, dz, oz) exactly), clamps with it
     ConeRay r = ray;
@@ -455,8 +467,8 @@ __global__ void __launch_bounds__(PB_X *PB_Y, 4)
     cone_fp_padded_kernel(const T *__restrict__ xfast, const T *__restrict__ yfast,
                           const typename Cell<T>::type *__restrict__ cells, Tout *__restrict__ sino,
                           const ConeFpView *__restrict__ views, const float *__restrict__ step_ptr,
-                          const float *__restrict__ spacing_ptr, int X, int Y, int Z, int W, int H, int n_proj,
-                          int geom_batch, int b, const unsigned *__restrict__ flags)
+                          const float *__restrict__ spacing_ptr, int X, int Y, int Z, int cell_sx, int W, int H,
+                          int n_proj, int geom_batch, int b, const unsigned *__restrict__ flags)
 {
     __shared__ float out_tile[PB_Y][PB_X + 1];
     const RayBlock rb = ray_block(blockIdx.x, W, H, n_proj);
@@ -485,9 +497,9 @@ __global__ void __launch_bounds__(PB_X *PB_Y, 4)
         const int Xp = X + 3, Yp = Y + 3;
         if (zmode) {
             if (packed)
-                pixel = march_cells<T, sizeof(T) == 2>(ray, step, inside, cells, Y, Z, xmax, ymax, zmax);
+                pixel = march_cells<T, sizeof(T) == 2>(ray, step, inside, cells, Z, cell_sx, xmax, ymax, zmax);
             else
-                pixel = march_cells<T, false>(ray, step, inside, cells, Y, Z, xmax, ymax, zmax);
+                pixel = march_cells<T, false>(ray, step, inside, cells, Z, cell_sx, xmax, ymax, zmax);
         } else {
             // rays mostly along x -> y-fastest copy
             const double cr0 = view.inv_ar[2] + 0.5 * (W - 1) * view.inv_ar[0] + 0.5 * (H - 1) * view.inv_ar[1];
@@ -522,6 +534,26 @@ size_t section_bytes(size_t n)
     return (n + 255) / 256 * 256;
 }
 
+// x pitch (in cells) of the cell copy: the least s_x >= (Y+2) (Z+2) for which
+// the sampler's biased index, cell_index_bias + index, stays in [0, 2^32) for
+// every index of the copy relative to floor (0, 0, 0) -- from -(s_x + s_y + 1)
+// up to below (X+2) s_x -- under both z floors; 0 when none is found.  The
+// bias moves by FLOOR_BIAS (mod 2^32) per unit of s_x, which steps through all
+// 1024 multiples of 2^22, so a few units of padding suffice.
+long long cell_x_pitch(int vol_x, int vol_y, int vol_z)
+{
+    const unsigned long long Xc = vol_x + 2, Yc = vol_y + 2, Zc = vol_z + 2;
+    for (unsigned long long sx = Yc * Zc; sx < Yc * Zc + 2048 && Xc * sx < (1ULL << 31); ++sx) {
+        bool ok = true;
+        for (const bool z2 : {false, true}) {
+            const unsigned long long bias = cell_index_bias((unsigned)sx, (unsigned)Zc, z2);
+            ok = ok && bias >= sx + Zc + 1 && bias + Xc * sx <= (1ULL << 32);
+        }
+        if (ok) return (long long)sx;
+    }
+    return 0;
+}
+
 template <typename Tin, typename Tout>
 cudaError_t launch_typed(const void *volume, void *sinogram, const Dims3D &d, const ConeFpView *views,
                          const float *step, const float *spacing, void *scratch, unsigned *flags, cudaStream_t stream)
@@ -529,6 +561,8 @@ cudaError_t launch_typed(const void *volume, void *sinogram, const Dims3D &d, co
     using CellT = typename Cell<Tin>::type;
     const size_t Xp = d.vol_x + 3, Yp = d.vol_y + 3, Zp = d.vol_z + 3;
     const size_t Xc = d.vol_x + 2, Yc = d.vol_y + 2, Zc = d.vol_z + 2;
+    const long long cell_sx = cell_x_pitch(d.vol_x, d.vol_y, d.vol_z);
+    if (cell_sx <= 0) return cudaErrorInvalidValue;
     char *base = (char *)scratch;
     Tin *xfast = (Tin *)base;
     Tin *yfast = (Tin *)(base + section_bytes(Xp * Yp * Zp * sizeof(Tin)));
@@ -545,11 +579,12 @@ cudaError_t launch_typed(const void *volume, void *sinogram, const Dims3D &d, co
     for (int b = 0; b < d.batch; ++b) {
         const Tin *src = (const Tin *)volume + (size_t)b * d.vol_z * d.vol_y * d.vol_x;
         pad_volume_kernel<Tin><<<pgrid, pblock, 0, stream>>>(src, xfast, yfast, d.vol_x, d.vol_y, d.vol_z, flags);
-        pad_cells_kernel<Tin><<<cgrid, pblock, 0, stream>>>(src, cells, d.vol_x, d.vol_y, d.vol_z, flags);
+        pad_cells_kernel<Tin><<<cgrid, pblock, 0, stream>>>(src, cells, d.vol_x, d.vol_y, d.vol_z, (int)cell_sx,
+                                                             flags);
         cone_fp_padded_kernel<Tin, Tout><<<grid, block, 0, stream>>>(xfast, yfast, cells, (Tout *)sinogram, views,
                                                                      step, spacing, d.vol_x, d.vol_y, d.vol_z,
-                                                                     d.det_w, d.det_h, d.n_proj, d.geom_batch, b,
-                                                                     flags);
+                                                                     (int)cell_sx, d.det_w, d.det_h, d.n_proj,
+                                                                     d.geom_batch, b, flags);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
@@ -562,7 +597,7 @@ size_t cone_fp_padded_scratch_bytes(int vol_z, int vol_y, int vol_x, int in_dtyp
 {
     const size_t e = dtype_size(in_dtype);
     const size_t padded = (size_t)(vol_x + 3) * (vol_y + 3) * (vol_z + 3);
-    const size_t cells = (size_t)(vol_x + 2) * (vol_y + 2) * (vol_z + 2);
+    const size_t cells = (size_t)(vol_x + 2) * (size_t)cell_x_pitch(vol_x, vol_y, vol_z);
     return 2 * section_bytes(padded * e) + section_bytes(cells * 8 * e);
 }
 
@@ -570,7 +605,7 @@ bool cone_fp_padded_supported(const Dims3D &d)
 {
     const long long padded = (long long)(d.vol_x + 3) * (d.vol_y + 3) * (d.vol_z + 3);
     return padded < (1LL << 31) - (1LL << 20) && ray_blocks_fit(d.det_w, d.det_h, d.n_proj) &&
-           d.vol_z + 3 <= 65535 && d.vol_y + 3 <= 65535;
+           d.vol_z + 3 <= 65535 && d.vol_y + 3 <= 65535 && cell_x_pitch(d.vol_x, d.vol_y, d.vol_z) > 0;
 }
 
 cudaError_t launch_cone_fp_padded(const void *volume, void *sinogram, int in_dtype, int out_dtype, const Dims3D &d,
