@@ -67,14 +67,14 @@ NCU_DRAM_BYTES = {
 }
 # ncu counters of the forward kernel from a section capture of its first
 # launch at 256^3 (issue activity, lanes, instructions per ray sample; L2 ->
-# SM bytes per ray sample from a --set full capture at 256^3, scaling with the
-# sample count)
+# SM bytes per ray sample from the same capture, scaling with the sample
+# count)
 NCU_FORWARD_COUNTERS = {
     ("cone512", "fp16", "fp16", False): {
-        "issue_active": 0.805, "lanes_active_per_warp_instruction": 26.71,
-        "thread_instructions_per_sample": 36.2, "lts2xbar_bytes_per_sample_256": 11.0,
+        "issue_active": 0.787, "lanes_active_per_warp_instruction": 26.74,
+        "thread_instructions_per_sample": 34.1, "lts2xbar_bytes_per_sample_256": 10.9,
         "source": "profiles/cone_fp_padded_kernel_cone256_fp16.md (256^3 capture; L2 -> SM bytes per sample "
-                  "from the full capture, scaling with the samples)"},
+                  "from its L2 read sectors of the texture unit, scaling with the samples)"},
 }
 # kernels of ours launched per fwd+back step (geometry preparation, view
 # classification, the two volume copies, forward; preparation, backprojection)
