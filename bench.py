@@ -63,7 +63,7 @@ PHANTOM_ELLIPSOIDS = 32
 #   python bench.py --steps 1 --warmup 3 --no-cpu-baseline
 # keyed by (workload, volume storage, sinogram storage, hardware_interp)
 NCU_DRAM_BYTES = {
-    ("cone512", "fp16", "fp16", False): 38.485e9 + 0.573e9,
+    ("cone512", "fp16", "fp16", False): 37.231e9 + 0.571e9,
 }
 # ncu counters of the forward kernel from a section capture of its first
 # launch at 256^3 (issue activity, lanes, instructions per ray sample; L2 ->
