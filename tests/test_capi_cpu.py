@@ -59,6 +59,39 @@ def test_workspace_sizes():
     assert lib.pyronn_cone_projection3d_workspace_size(1, 8, 8, 8, 10, 4, 4, 9, 0, 1) == 0
 
 
+def _cell_pitch(vol_x, vol_y, vol_z):
+    """x pitch of the forward's cell copy: the least s_x >= (Y+2)(Z+2) for
+    which the sampler's floor-biased cell index (bias 0x4B400000 per unit of
+    the x and y strides plus the z floor's bias, 0x4B400000 or, for z in
+    half-voxel units, 0x4BC00000; mod 2^32) plus any index of the copy stays
+    in [0, 2^32)."""
+    xc, yc, zc = vol_x + 2, vol_y + 2, vol_z + 2
+    sx = yc * zc
+    while True:
+        biases = [(0x4B400000 * (sx + zc) + zb) % 2 ** 32 for zb in (0x4B400000, 0x4BC00000)]
+        if all(b >= sx + zc + 1 and b + xc * sx <= 2 ** 32 for b in biases):
+            return sx
+        sx += 1
+
+
+def test_cell_copy_pitch():
+    """The forward's workspace holds the cell copy at the pitch its index
+    arithmetic needs: (Y+2)(Z+2) cells for most shapes, one more where the
+    biased index would otherwise wrap (vol 91 x 8 x 196, z y x)."""
+    lib = _capi.load()
+
+    def align(n):
+        return (n + 255) // 256 * 256
+    for z, y, x in [(64, 64, 64), (91, 8, 196), (512, 512, 512), (85, 150, 38)]:
+        sx = _cell_pitch(x, y, z)
+        fp16 = lib.pyronn_cone_projection3d_workspace_size(1, z, y, x, 16, 40, 60, 1, 0, 1)
+        fp_hw = lib.pyronn_cone_projection3d_workspace_size(1, z, y, x, 16, 40, 60, 1, 1, 1)
+        padded = (x + 3) * (y + 3) * (z + 3)
+        assert fp16 - fp_hw == 2 * align(padded * 2) + align((x + 2) * sx * 16)
+    assert _cell_pitch(196, 8, 91) == 10 * 93 + 1
+    assert _cell_pitch(64, 64, 64) == 66 * 66
+
+
 FAKE = 4096  # non-null, never dereferenced: validation fails first
 
 

@@ -527,6 +527,21 @@ def test_cone_projection_wide_fp16_range(cuda):
     assert rel_l2(out.cpu().numpy(), ref) < 2e-5
 
 
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float16])
+def test_cone_projection_padded_cell_pitch(cuda, dtype):
+    """A volume (91 x 8 x 196, z y x) whose cell copy needs one cell of x
+    pitch padding for the sampler's biased index not to wrap: the forward
+    over that layout matches the oracle."""
+    geo = geometry.ConeBeam3D((91, 8, 196), (1.0, 1.0, 1.0), (40, 60), (3.0, 3.0), 8, 300.0, 500.0,
+                              step_size=0.5, projection_multiplier=0.8)
+    vol = phantoms.ellipsoid_phantom_3d(geo.volume_shape, geo.volume_spacing, seed=9, n=6)[0][None]
+    x = t(vol, cuda, dtype)
+    out = pl.cone_projection3d(x, geo.detector_shape, *geo.args(), out_dtype=torch.float32)
+    ref = oracle.cone_projection3d(rounded(x), geo.detector_shape, *geo.args())
+    assert (ref != 0).any()
+    assert rel_l2(out.cpu().numpy(), ref) < CONE_FWD_TOL[dtype]
+
+
 # ------------------------------------------------------------ device geometry
 
 
