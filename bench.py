@@ -5,8 +5,8 @@
                     [--workload cone512|cone256] [--storage bf16|fp16|fp32]
 
 One step = ConeProjection3D of a 512^3 (or 256^3) volume followed by
-ConeBackprojection3D of the resulting sinogram (360 views), the north-star
-workload.  GUPS = 2 U / t with U = voxels x views (the update count of one
+ConeBackprojection3D of the resulting sinogram (360 views), 1024 x 768
+detector, the headline workload.  GUPS = 2 U / t with U = voxels x views (the update count of one
 backprojection, used for both directions as the metric defines it).
 
 * ``value``: device-resident inputs, CUDA events around exactly K steps,
