@@ -90,6 +90,9 @@ def test_cell_copy_pitch():
         assert fp16 - fp_hw == 2 * align(padded * 2) + align((x + 2) * sx * 16)
     assert _cell_pitch(196, 8, 91) == 10 * 93 + 1
     assert _cell_pitch(64, 64, 64) == 66 * 66
+    # padded copies past 2^31 elements: the direct path, which needs no copies
+    big = [lib.pyronn_cone_projection3d_workspace_size(1, 1300, 1300, 1300, 16, 40, 60, 1, hw, 1) for hw in (0, 1)]
+    assert big[0] == big[1] > 0
 
 
 FAKE = 4096  # non-null, never dereferenced: validation fails first
