@@ -155,14 +155,18 @@ struct Cell16 {
     // 11 instructions for the seven lerps instead of 16.  Differences of the
     // interpolated pair must fit the storage type: used when every input
     // magnitude is below Wide16<T16>::limit (FLAG_WIDE clear).
-    // (tz2 = 2 tz, the z weight in half-voxel units)
+    // (tz2 = 2 tz, the z weight in half-voxel units).  Both weights are
+    // rounded by one conversion into the two halves of a word and each packed
+    // FMA takes its half replicated: 512^3 FP16 forward 77.3 -> 75.4 ms
+    // against one conversion per weight (the same bits)
     __device__ static float trilinear_packed(const uint4 *c, float tz2f, float ty, float tx)
     {
         const uint4 w = __ldg(c);
         unsigned tz2, ty2, zy0, zy1, dy, yv;
         if (BF16) {
-            asm("cvt.rn.bf16x2.f32 %0, %1, %1;" : "=r"(tz2) : "f"(tz2f));
-            asm("cvt.rn.bf16x2.f32 %0, %1, %1;" : "=r"(ty2) : "f"(ty));
+            asm("{.reg .b32 p; .reg .b16 l, h; cvt.rn.bf16x2.f32 p, %2, %3; mov.b32 {l, h}, p; mov.b32 %0, {l, l};"
+                " mov.b32 %1, {h, h};}"
+                : "=r"(tz2), "=r"(ty2) : "f"(ty), "f"(tz2f));
             asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(zy0) : "r"(tz2), "r"(w.y), "r"(w.x));
             asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(zy1) : "r"(tz2), "r"(w.w), "r"(w.z));
             asm("sub.rn.bf16x2 %0, %1, %2;" : "=r"(dy) : "r"(zy1), "r"(zy0));
@@ -170,8 +174,9 @@ struct Cell16 {
             const float lo = __uint_as_float(yv << 16);
             return fmaf(tx, sub_f32_bf16<true>(yv, lo), lo);
         } else {
-            asm("cvt.rn.f16x2.f32 %0, %1, %1;" : "=r"(tz2) : "f"(tz2f));
-            asm("cvt.rn.f16x2.f32 %0, %1, %1;" : "=r"(ty2) : "f"(ty));
+            asm("{.reg .b32 p; .reg .b16 l, h; cvt.rn.f16x2.f32 p, %2, %3; mov.b32 {l, h}, p; mov.b32 %0, {l, l};"
+                " mov.b32 %1, {h, h};}"
+                : "=r"(tz2), "=r"(ty2) : "f"(ty), "f"(tz2f));
             asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(zy0) : "r"(tz2), "r"(w.y), "r"(w.x));
             asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(zy1) : "r"(tz2), "r"(w.w), "r"(w.z));
             asm("sub.rn.f16x2 %0, %1, %2;" : "=r"(dy) : "r"(zy1), "r"(zy0));
