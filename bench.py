@@ -740,9 +740,11 @@ def run_ours(args, cfg):
                            "streams during step i's projections; every step's input and result cross the host "
                            "link inside the timed region"},
         # (+1 per step where the backprojection pairs a 16-bit sinogram: at
-        # least 100 voxels per detector pixel)
+        # least 100 voxels per detector pixel; +1 where the forward scans a
+        # 16-bit volume's range before its cell copy)
         "gpu_launches": (LAUNCHES_PER_STEP[hw] + int(not hw and sino_storage != torch.float32
-                                                    and Z * Y * X >= 100 * H * W)) * args.steps,
+                                                    and Z * Y * X >= 100 * H * W)
+                         + int(not hw and args.storage != "fp32")) * args.steps,
         "clocks": clocks,
     }
 

@@ -148,13 +148,14 @@ struct Cell16 {
         zlerp(c, tz, zl);
         return lerp_ref(lerp_ref(zl[0], zl[2], ty), lerp_ref(zl[1], zl[3], ty), tx);
     }
-    // Packed: the z lerps of the (x0, x1) pairs at y0 and at y1 as two FMAs
-    // on pairs of 16-bit values (z0 + (2t) hd, one rounding each), the y lerp
-    // of the pair as a packed difference and FMA, the x lerp in FP32 on the
-    // pair widened (one widening, one mixed-precision subtraction, one FMA):
-    // 11 instructions for the seven lerps instead of 16.  Differences of the
-    // interpolated pair must fit the storage type: used when every input
-    // magnitude is below Wide16<T16>::limit (FLAG_WIDE clear).
+    // Packed, on the y-difference cells (make_ydiff): the z lerp of the
+    // (x0, x1) pair at y0 as one FMA on pairs of 16-bit values (z0 + (2t) hd,
+    // one rounding), the pair's y difference -- z lerp at y1 minus z lerp at
+    // y0 -- as one FMA on the cell's y-difference words (Dz0 + (2t) Dhd), the
+    // y lerp as one FMA, the x lerp in FP32 on the pair widened (one widening,
+    // one mixed-precision subtraction, one FMA): 7 instructions for the seven
+    // lerps.  The differences must fit the storage type: used when every input
+    // magnitude is below Wide16<T16>'s bound (FLAG_WIDE clear).
     // (tz2 = 2 tz, the z weight in half-voxel units).  Both weights are
     // rounded by one conversion into the two halves of a word and each packed
     // FMA takes its half replicated: 512^3 FP16 forward 77.3 -> 75.4 ms
@@ -162,14 +163,13 @@ struct Cell16 {
     __device__ static float trilinear_packed(const uint4 *c, float tz2f, float ty, float tx)
     {
         const uint4 w = __ldg(c);
-        unsigned tz2, ty2, zy0, zy1, dy, yv;
+        unsigned tz2, ty2, zy0, dy, yv;
         if (BF16) {
             asm("{.reg .b32 p; .reg .b16 l, h; cvt.rn.bf16x2.f32 p, %2, %3; mov.b32 {l, h}, p; mov.b32 %0, {l, l};"
                 " mov.b32 %1, {h, h};}"
                 : "=r"(tz2), "=r"(ty2) : "f"(ty), "f"(tz2f));
             asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(zy0) : "r"(tz2), "r"(w.y), "r"(w.x));
-            asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(zy1) : "r"(tz2), "r"(w.w), "r"(w.z));
-            asm("sub.rn.bf16x2 %0, %1, %2;" : "=r"(dy) : "r"(zy1), "r"(zy0));
+            asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(dy) : "r"(tz2), "r"(w.w), "r"(w.z));
             asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(yv) : "r"(ty2), "r"(dy), "r"(zy0));
             const float lo = __uint_as_float(yv << 16);
             return fmaf(tx, sub_f32_bf16<true>(yv, lo), lo);
@@ -178,8 +178,7 @@ struct Cell16 {
                 " mov.b32 %1, {h, h};}"
                 : "=r"(tz2), "=r"(ty2) : "f"(ty), "f"(tz2f));
             asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(zy0) : "r"(tz2), "r"(w.y), "r"(w.x));
-            asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(zy1) : "r"(tz2), "r"(w.w), "r"(w.z));
-            asm("sub.rn.f16x2 %0, %1, %2;" : "=r"(dy) : "r"(zy1), "r"(zy0));
+            asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(dy) : "r"(tz2), "r"(w.w), "r"(w.z));
             asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(yv) : "r"(ty2), "r"(dy), "r"(zy0));
             const float lo = __half2float(__ushort_as_half((unsigned short)(yv & 0xFFFFu)));
             return fmaf(tx, sub_f32_f16<true>(yv, lo), lo);
@@ -200,6 +199,27 @@ struct Cell16 {
         const unsigned w3 = (unsigned)half_diff(v[6], v[4]) | ((unsigned)half_diff(v[7], v[5]) << 16);
         return make_uint4(w0, w1, w2, w3);
     }
+    __device__ static float value(unsigned short b)
+    {
+        if constexpr (BF16)
+            return __bfloat162float(__ushort_as_bfloat16(b));
+        else
+            return __half2float(__ushort_as_half(b));
+    }
+    // b - a for each half of two words: exact in FP32, one rounding each
+    __device__ static unsigned word_diff(unsigned b, unsigned a)
+    {
+        const unsigned short lo = bits(T16(value((unsigned short)b) - value((unsigned short)a)));
+        const unsigned short hi = bits(T16(value((unsigned short)(b >> 16)) - value((unsigned short)(a >> 16))));
+        return (unsigned)lo | ((unsigned)hi << 16);
+    }
+    // the packed lerps' cells: the y0 words of make, then the y1 words minus
+    // the y0 words (z0 taps, half-differences), rounded to the storage type
+    __device__ static uint4 make_ydiff(const T16 (&v)[8])
+    {
+        const uint4 c = make(v);
+        return make_uint4(c.x, c.y, word_diff(c.z, c.x), word_diff(c.w, c.y));
+    }
 };
 template <>
 struct Cell<__nv_bfloat16> : Cell16<__nv_bfloat16> {
@@ -207,16 +227,18 @@ struct Cell<__nv_bfloat16> : Cell16<__nv_bfloat16> {
 template <>
 struct Cell<__half> : Cell16<__half> {
 };
-// Magnitudes above which the packed lerps' differences of two interpolated
-// 16-bit values could leave the storage type's range (FP16: 2 x 32752 = 65504,
-// its largest finite value); FP32 input never takes the packed lerps.
+// Magnitudes above which the packed lerps' differences could leave the
+// storage type's range.  FP16: below L = 32704 every stored difference is at
+// most 2L and the y difference of two interpolated values, Dz0 + (2t) Dhd, at
+// most 2L plus its roundings (under 2.5 ulp of 2L = 80): 65488, inside the
+// largest finite value 65504.  FP32 input never takes the packed lerps.
 template <typename T>
 struct Wide16 {
     __device__ static bool exceeds(T) { return false; }
 };
 template <>
 struct Wide16<__half> {
-    __device__ static bool exceeds(__half v) { return fabsf(__half2float(v)) > 32752.0f; }
+    __device__ static bool exceeds(__half v) { return fabsf(__half2float(v)) > 32704.0f; }
 };
 template <>
 struct Wide16<__nv_bfloat16> {
@@ -233,6 +255,22 @@ struct Wide16<__nv_bfloat16> {
 // plane per block, 0.88 ms with four; the whole forward op 80.39 / 80.14 /
 // 80.10 ms with one / four / eight).  Skipped when no view is in z mode.
 constexpr int CELL_PLANES = 8;
+
+// Sets FLAG_WIDE when a 16-bit input holds a magnitude beyond Wide16's bound:
+// the cell copy then keeps the plain cells (z0 taps at y1, not differences)
+// and the rays take FP32 y and x lerps.  One read of the volume before the
+// copy, whose cell form depends on it.
+template <typename T>
+__global__ void __launch_bounds__(256) detect_wide_kernel(const T *__restrict__ src, size_t n,
+                                                          unsigned *__restrict__ flags)
+{
+    if (!flags[FLAG_NEED_Z]) return;
+    bool wide = false;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        wide |= Wide16<T>::exceeds(src[i]);
+    if (__syncthreads_or(wide) && threadIdx.x == 0) atomicOr(&flags[FLAG_WIDE], 1u);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(PAD_TILE *8) pad_cells_kernel(const T *__restrict__ src,
                                                                  typename Cell<T>::type *__restrict__ dst, int X,
@@ -241,7 +279,8 @@ __global__ void __launch_bounds__(PAD_TILE *8) pad_cells_kernel(const T *__restr
     if (!flags[FLAG_NEED_Z]) return;
     // [y - (yc0-1)][z - (zc0-1)][x - (xc0-1)]
     __shared__ T tile[CELL_PLANES + 1][PAD_TILE + 1][PAD_TILE + 2];
-    bool wide = false;
+    // 16-bit inputs within range take the packed lerps' y-difference cells
+    const bool ydiff = sizeof(T) == 2 && !flags[FLAG_WIDE];
     const int Yc = Y + 2, Zc = Z + 2;
     const int xc0 = blockIdx.x * PAD_TILE, yc0 = blockIdx.y * CELL_PLANES, zc0 = blockIdx.z * PAD_TILE;
     for (int rr = threadIdx.y; rr < (CELL_PLANES + 1) * (PAD_TILE + 1); rr += 8) {
@@ -252,11 +291,10 @@ __global__ void __launch_bounds__(PAD_TILE *8) pad_cells_kernel(const T *__restr
             const int x = xc0 - 1 + c;
             T v = T(0.0f);
             if (yz_in && x >= 0 && x < X) v = src[((size_t)z * Y + y) * X + x];
-            wide |= Wide16<T>::exceeds(v);
             tile[dy][r][c] = v;
         }
     }
-    if (__syncthreads_or(wide) && threadIdx.x == 0 && threadIdx.y == 0) atomicOr(&flags[FLAG_WIDE], 1u);
+    __syncthreads();
     const int tz = threadIdx.x, zc = zc0 + tz;
     if (zc >= Zc) return;
 #pragma unroll
@@ -270,7 +308,12 @@ __global__ void __launch_bounds__(PAD_TILE *8) pad_cells_kernel(const T *__restr
                 const T v[8] = {tile[pl][tz][c],     tile[pl][tz][c + 1],     tile[pl][tz + 1][c],
                                 tile[pl][tz + 1][c + 1], tile[pl + 1][tz][c], tile[pl + 1][tz][c + 1],
                                 tile[pl + 1][tz + 1][c], tile[pl + 1][tz + 1][c + 1]};
-                dst[(size_t)xc * s_x + (size_t)yc * Zc + zc] = Cell<T>::make(v);
+                typename Cell<T>::type cell;
+                if constexpr (sizeof(T) == 2)
+                    cell = ydiff ? Cell<T>::make_ydiff(v) : Cell<T>::make(v);
+                else
+                    cell = Cell<T>::make(v);
+                dst[(size_t)xc * s_x + (size_t)yc * Zc + zc] = cell;
             }
         }
     }
@@ -584,6 +627,11 @@ cudaError_t launch_typed(const void *volume, void *sinogram, const Dims3D &d, co
     for (int b = 0; b < d.batch; ++b) {
         const Tin *src = (const Tin *)volume + (size_t)b * d.vol_z * d.vol_y * d.vol_x;
         pad_volume_kernel<Tin><<<pgrid, pblock, 0, stream>>>(src, xfast, yfast, d.vol_x, d.vol_y, d.vol_z, flags);
+        if constexpr (sizeof(Tin) == 2) {
+            const size_t n = (size_t)d.vol_z * d.vol_y * d.vol_x;
+            const unsigned wgrid = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 8);
+            detect_wide_kernel<Tin><<<wgrid, 256, 0, stream>>>(src, n, flags);
+        }
         pad_cells_kernel<Tin><<<cgrid, pblock, 0, stream>>>(src, cells, d.vol_x, d.vol_y, d.vol_z, (int)cell_sx,
                                                              flags);
         cone_fp_padded_kernel<Tin, Tout><<<grid, block, 0, stream>>>(xfast, yfast, cells, (Tout *)sinogram, views,
