@@ -37,8 +37,9 @@ constexpr int PB_Y = 8;
 constexpr int PAD_TILE = 32;
 constexpr size_t PAD_Z_BLOCKS = 16;  // z blocks of the xy-mode padded copy, each striding over planes
 // workspace header words (after the error flag) set by classify_views_kernel
-// (FLAG_WIDE: a 16-bit input holds magnitudes whose differences may not fit
-// the storage type, so the cells take the FP32 y and x lerps)
+// (FLAG_WIDE, set by detect_wide_kernel: a 16-bit input holds magnitudes
+// whose differences may not fit the storage type, so the cells keep their
+// plain form and the rays take the FP32 y and x lerps)
 enum { FLAG_NEED_XY = 1, FLAG_NEED_Z = 2, FLAG_WIDE = 3 };
 
 __global__ void classify_views_kernel(const ConeFpView *__restrict__ views, int n, unsigned *__restrict__ flags)
@@ -58,10 +59,13 @@ __global__ void classify_views_kernel(const ConeFpView *__restrict__ views, int 
 // of the z0 tap (sm_100 fma.f32.f16 / add.f32.f16, bf16 alike), or, in the
 // packed form used unless the input's range forbids it, as a packed FMA on
 // the (x0, x1) pair, followed by the pair's y lerp in packed form and the x
-// lerp in FP32 (trilinear_packed).  Roundings to the storage type happen only
-// where neighbouring taps differ: the 512^3 forward's error against the FP64
+// lerp in FP32 (trilinear_packed); the packed form's cells hold their y1
+// words as differences from the y0 words (make_ydiff), so the y difference
+// of the pair is one FMA.  Roundings to the storage type happen only where
+// neighbouring taps differ: the 512^3 forward's error against the FP64
 // oracle stays the storage rounding's (FP16 2.65e-4), measured at 96.8 ms
-// (widened taps, FP32 lerps) -> 90.0 ms (mixed z lerps) -> 83.0 ms (packed).
+// (widened taps, FP32 lerps) -> 90.0 ms (mixed z lerps) -> 83.0 ms (packed)
+// -> 75.4 ms (other changes) -> 73.0 ms (y-difference cells).
 struct alignas(16) CellF32 {
     float4 y0, y1;  // (x0 z0, x1 z0, x0 z1, x1 z1) at y0, then at y1
 };
@@ -125,7 +129,8 @@ struct Cell<float> {
     }
 };
 // the 16-bit cells: words (z0 taps at y0, half-differences at y0, z0 taps
-// at y1, half-differences at y1)
+// at y1, half-differences at y1) -- or, for the packed lerps, the last two
+// as their differences from the first two (make_ydiff)
 template <typename T16>
 struct Cell16 {
     static constexpr bool BF16 = std::is_same<T16, __nv_bfloat16>::value;

@@ -513,8 +513,8 @@ def test_cone_projection_volume_partly_off_detector(cuda, hw):
 
 def test_cone_projection_wide_fp16_range(cuda):
     """FP16 inputs whose magnitudes could overflow FP16 in the packed lerps'
-    differences (above 32752) take FP32 y and x lerps: the cell copy flags
-    them, and the result matches the oracle as closely as a normal-range
+    differences (above 32704) take FP32 y and x lerps: a scan of the input
+    before the cell copy flags them, and the result matches the oracle as closely as a normal-range
     input's.  (The BF16 bound, 8.5e37, lies beyond what FP32 sums of a ray can
     hold anyway.)"""
     geo = _cone_geo()
