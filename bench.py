@@ -71,8 +71,8 @@ NCU_DRAM_BYTES = {
 # count)
 NCU_FORWARD_COUNTERS = {
     ("cone512", "fp16", "fp16", False): {
-        "issue_active": 0.781, "lanes_active_per_warp_instruction": 26.75,
-        "thread_instructions_per_sample": 33.1, "lts2xbar_bytes_per_sample_256": 11.0,
+        "issue_active": 0.781, "lanes_active_per_warp_instruction": 26.77,
+        "thread_instructions_per_sample": 32.1, "lts2xbar_bytes_per_sample_256": 11.1,
         "source": "profiles/cone_fp_padded_kernel_cone256_fp16.md (256^3 capture; L2 -> SM bytes per sample "
                   "from its L2 read sectors of the texture unit, scaling with the samples)"},
 }
